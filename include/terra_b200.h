@@ -1,0 +1,125 @@
+/*
+ * terra_b200 -- C ABI of the B200-native TERRA-NG Stokes hot path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * an int status (TN_OK == 0, negative on error; tn_last_error() describes the
+ * last failure of the calling thread). Array arguments named *_dev are device
+ * pointers; they must be 16-byte aligned (cudaMalloc / torch allocations are).
+ * Operations run asynchronously on the caller's CUDA stream (NULL = legacy
+ * default stream) unless documented as synchronous.
+ *
+ * Data layout is the reference's diamond-grid layout (src/terra/grid/
+ * grid_types.hpp:12-113, Kokkos::LayoutRight): a nodal scalar field is
+ * (10, nl, nl, nr) with r fastest; a velocity field is three such arrays (the
+ * SoA Grid4DDataVec); lateral coordinates are (10, nl, nl, 3); cell fields
+ * are (10, nl-1, nl-1, nr-1). Level indices count from 0 (coarsest).
+ *
+ * Each declaration names the reference interface it replaces (paths inside the
+ * reference project).
+ */
+#ifndef TERRA_B200_H
+#define TERRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status, enums -------------------------------------------------------- */
+enum {
+    TN_OK               = 0,
+    TN_ERR_ARG          = -1, /* invalid argument (extent mismatch, bad pointer, ...) */
+    TN_ERR_CUDA         = -2, /* CUDA runtime error */
+    TN_ERR_ALLOC        = -3, /* device allocation failed */
+    TN_ERR_STATE        = -4, /* object not in a state that allows the call */
+    TN_ERR_DEVICE       = -5, /* a kernel reported a device-side error (bounded wait expired) */
+    TN_ERR_UNSUPPORTED  = -6, /* option combination not implemented */
+    TN_ERR_NOT_CONVERGED = -7 /* iterative solve stopped before reaching its tolerance */
+};
+enum { TN_F64 = 0, TN_F32 = 1 };
+/* BoundaryConditionFlag (src/terra/grid/shell/bit_masks.hpp:20-25) */
+enum { TN_NEUMANN = 0, TN_DIRICHLET = 1, TN_FREESLIP = 2 };
+/* OperatorApplyMode / OperatorCommunicationMode (src/terra/linalg/operator.hpp:29-51) */
+enum { TN_REPLACE = 0, TN_ADD = 1 };
+enum { TN_SKIP_COMMUNICATION = 0, TN_COMMUNICATE_ADDITIVELY = 1 };
+
+typedef struct tn_shell    tn_shell;
+typedef struct tn_operator tn_operator;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* tn_last_error(void);
+/* Library version string. */
+const char* tn_version(void);
+
+/* ---- mesh hierarchy --------------------------------------------------------
+ * Replaces DistributedDomain / DomainInfo with one subdomain per diamond plus
+ * subdomain_unit_sphere_single_shell_coords, subdomain_shell_radii and the
+ * boundary / ownership masks (src/terra/grid/shell/spherical_shell.hpp:825-2967,
+ * src/terra/grid/shell/bit_masks.hpp:82-136, src/terra/grid/bit_masks.hpp:27-85).
+ * Builds num_levels levels; level num_levels-1 has lateral refinement
+ * lat_level and radial refinement rad_level (2^rad_level layers), each coarser
+ * level halves both. Uniform radii in [r_min, r_max]. Synchronous.          */
+int tn_shell_create(int lat_level, int rad_level, int num_levels, double r_min, double r_max, tn_shell** out);
+void tn_shell_destroy(tn_shell* shell);
+int tn_shell_num_levels(const tn_shell* shell, int* num_levels);
+int tn_shell_level_dims(const tn_shell* shell, int level, int* nl, int* nr);
+/* Host copies (synchronous). coords (10,nl,nl,3); radii (nr); ownership and
+ * boundary mask (10,nl,nl,nr) as uint8 flags (NodeOwnershipFlag,
+ * ShellBoundaryFlag values); class_of_lat (10,nl,nl): duplicate-node class or -1. */
+int tn_shell_copy_coords(const tn_shell* shell, int level, double* coords_host);
+int tn_shell_copy_radii(const tn_shell* shell, int level, double* radii_host);
+int tn_shell_copy_ownership(const tn_shell* shell, int level, uint8_t* owned_host);
+int tn_shell_copy_boundary_mask(const tn_shell* shell, int level, uint8_t* mask_host);
+int tn_shell_duplicate_classes(const tn_shell* shell, int level, int32_t* class_of_lat_host, int* num_classes);
+/* Host-only mesh generation of one level (no device needed): the same
+ * generator tn_shell_create uses. Any output pointer may be NULL. Shapes:
+ * coords (10,nl,nl,3), radii (nr), owned (10,nl,nl), class_of_lat (10,nl,nl). */
+int tn_mesh_generate_host(int lat_level, int rad_level, double r_min, double r_max, double* coords_host,
+                          double* radii_host, uint8_t* owned_lat_host, int32_t* class_of_lat_host, int* num_classes);
+/* Device error word written by bounded waits inside kernels (0 = none);
+ * reading it synchronizes the device and clears it. */
+int tn_shell_check_device_error(tn_shell* shell, int* code);
+
+/* ---- epsilon-div-div operator ----------------------------------------------
+ * Replaces EpsilonDivDivKerngen<ScalarT> (src/terra/fe/wedge/operators/shell/
+ * epsilon_divdiv_kerngen.hpp:205-216 constructor, :447-528 setters, :577-792
+ * apply_impl). Exactly one of k_nodal_dev (10,nl,nl,nr) or k_cell_dev
+ * (10,nl-1,nl-1,nr-1; set_q0_coefficient_field) is non-NULL; it is copied.
+ * Arrays are in the operator's precision (TN_F64 / TN_F32). Defaults:
+ * Replace + CommunicateAdditively. Requires a level with at least 2 layers. */
+int tn_epsdivdiv_create(tn_shell* shell, int level, int precision, const void* k_nodal_dev, const void* k_cell_dev,
+                        int bc_cmb, int bc_surface, int diagonal, tn_operator** out);
+void tn_operator_destroy(tn_operator* op);
+/* set_operator_apply_and_communication_modes (epsilon_divdiv_kerngen.hpp:447-453) */
+int tn_operator_set_modes(tn_operator* op, int apply_mode, int comm_mode);
+/* set_diagonal (epsilon_divdiv_kerngen.hpp:455) */
+int tn_operator_set_diagonal(tn_operator* op, int diagonal);
+/* set_boundary_conditions (epsilon_divdiv_kerngen.hpp:474-481) */
+int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surface);
+/* Override the CTA tile (0 = default); for tuning. */
+int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x);
+/* apply_impl: dst = A src (Replace) or dst += A src (Add); with
+ * CommunicateAdditively the interface duplicates are summed afterwards. src
+ * and dst are arrays of three device pointers (x, y, z components). */
+int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* dst_dev, void* stream);
+
+/* ---- nodal-vector kernels (VectorQ1Vec / VectorQ1Scalar, src/terra/linalg/
+ * vector_q1.hpp:20-304; kernels/common/grid_operations.hpp) --------------- */
+/* Sum every diamond-interface duplicate over its class (send_recv_with_plan,
+ * src/terra/communication/shell/communication_plan.hpp:48-71). */
+int tn_interface_sum(tn_shell* shell, int level, int precision, int ncomp, void* const* comps_dev, void* stream);
+/* y = c0 + sum_i c[i] x_i, nterms in 0..3 (lincomb, vector.hpp). */
+int tn_vec_lincomb(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, double c0, int nterms,
+                   const double* c, const void* const* x0_dev, const void* const* x1_dev, const void* const* x2_dev,
+                   void* stream);
+/* owned-node dot product accumulated in FP64 (masked_dot_product,
+ * grid_operations.hpp:630-673). Synchronous on `stream`. */
+int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev,
+               const void* const* b_dev, double* result, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TERRA_B200_H */

@@ -1,0 +1,533 @@
+"""CPU oracle for the TERRA-NG Stokes hot path -- TEST INFRASTRUCTURE ONLY.
+
+Python bindings to ``tn_oracle.c`` plus numpy restatements of the reference's
+solvers. Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
+baseline leg import this module; the product never does.
+
+Vector shapes: velocity ``(3, 10, nl, nl, nr)``, scalar ``(10, nl, nl, nr)``,
+cell fields ``(10, nl-1, nl-1, nr-1)``, all float64, r fastest.
+
+Reference citations are paths inside the reference project (src/terra/...).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libtn_oracle.so")
+_lib = None
+
+NEUMANN, DIRICHLET, FREESLIP = 0, 1, 2
+
+
+def build():
+    """Compile the oracle library (make, gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        dpp = ctypes.POINTER(dp)
+        L.tno_unit_sphere_coords.argtypes = [ctypes.c_int, dp]
+        L.tno_uniform_radii.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, dp]
+        L.tno_duplicate_classes.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]
+        L.tno_ownership.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint8)]
+        L.tno_boundary_mask.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8)]
+        for name in ("tno_epsdivdiv_slow", "tno_epsdivdiv_fast"):
+            getattr(L, name).argtypes = [ctypes.c_void_p, dpp, dpp]
+        L.tno_epsdivdiv_local_matrix.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [dp]
+        L.tno_epsdivdiv_stored.argtypes = [ctypes.c_void_p, dp, dpp, dpp]
+        L.tno_divergence.argtypes = [ctypes.c_void_p, dpp, dp]
+        L.tno_gradient.argtypes = [ctypes.c_void_p, dp, dpp]
+        L.tno_kmass_lumped.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
+        L.tno_vector_mass.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dpp, dpp]
+        L.tno_interface_sum.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp]
+        L.tno_prolongate_add.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
+        L.tno_restrict.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
+        L.tno_gca_coarsen.argtypes = [ctypes.c_void_p, dp, dp]
+        L.tno_masked_dot.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
+        L.tno_masked_dot.restype = ctypes.c_double
+        L.tno_epsdivdiv_vjp_logeta.argtypes = [ctypes.c_void_p, dpp, dpp, dp]
+        L.tno_set_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return lib().tno_set_threads(int(n))
+
+
+def _dp(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _dpp(arrs):
+    ptrs = (ctypes.POINTER(ctypes.c_double) * len(arrs))(*[_dp(a) for a in arrs])
+    return ptrs
+
+
+class _OpStruct(ctypes.Structure):
+    _fields_ = [
+        ("nl", ctypes.c_int),
+        ("nr", ctypes.c_int),
+        ("coords", ctypes.c_void_p),
+        ("radii", ctypes.c_void_p),
+        ("k", ctypes.c_void_p),
+        ("k_q0", ctypes.c_void_p),
+        ("bc_cmb", ctypes.c_int),
+        ("bc_surface", ctypes.c_int),
+        ("diagonal", ctypes.c_int),
+    ]
+
+
+# --------------------------------------------------------------------------
+# Mesh
+# --------------------------------------------------------------------------
+class Shell:
+    """One level of the thick spherical shell (grid/shell/spherical_shell.hpp)."""
+
+    def __init__(self, lat_level: int, rad_level: int | None = None, r_min=0.55, r_max=1.0):
+        if rad_level is None:
+            rad_level = lat_level
+        self.lat_level, self.rad_level = lat_level, rad_level
+        self.nl = (1 << lat_level) + 1
+        self.nr = (1 << rad_level) + 1
+        self.r_min, self.r_max = float(r_min), float(r_max)
+        L = lib()
+        self.coords = np.zeros((10, self.nl, self.nl, 3))
+        L.tno_unit_sphere_coords(lat_level, _dp(self.coords))
+        self.radii = np.zeros(self.nr)
+        L.tno_uniform_radii(self.r_min, self.r_max, self.nr, _dp(self.radii))
+        self.classes = np.zeros((10, self.nl, self.nl), np.int32)
+        self.num_classes = L.tno_duplicate_classes(lat_level, self.classes.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        self.owned_lat = np.zeros((10, self.nl, self.nl), np.uint8)
+        L.tno_ownership(lat_level, self.owned_lat.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        self.boundary_mask = np.zeros((10, self.nl, self.nl, self.nr), np.uint8)
+        L.tno_boundary_mask(self.nl, self.nr, self.boundary_mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        self.owned = np.broadcast_to(self.owned_lat[..., None], (10, self.nl, self.nl, self.nr)).astype(bool)
+
+    @property
+    def scalar_shape(self):
+        return (10, self.nl, self.nl, self.nr)
+
+    @property
+    def vec_shape(self):
+        return (3, 10, self.nl, self.nl, self.nr)
+
+    @property
+    def cell_shape(self):
+        return (10, self.nl - 1, self.nl - 1, self.nr - 1)
+
+    def coarser(self) -> "Shell":
+        return Shell(self.lat_level - 1, self.rad_level - 1, self.r_min, self.r_max)
+
+    def physical_coords(self):
+        """(10, nl, nl, nr, 3) node positions."""
+        return self.coords[:, :, :, None, :] * self.radii[None, None, None, :, None]
+
+    def interface_sum(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        comps = [v] if v.ndim == 4 else [v[i] for i in range(v.shape[0])]
+        comps = [np.ascontiguousarray(c) for c in comps]
+        lib().tno_interface_sum(self.lat_level, self.nr, len(comps), _dpp(comps))
+        return comps[0] if v.ndim == 4 else np.stack(comps)
+
+    def dot(self, a, b):
+        """Owned-masked dot (kernels/common/grid_operations.hpp:630-673)."""
+        m = self.owned
+        if a.ndim == 4:
+            return float(np.sum(a[m] * b[m]))
+        return float(sum(np.sum(a[i][m] * b[i][m]) for i in range(a.shape[0])))
+
+
+# --------------------------------------------------------------------------
+# Operators
+# --------------------------------------------------------------------------
+class EpsDivDiv:
+    """epsilon-div-div operator (epsilon_divdiv_kerngen.hpp), Replace mode,
+    interface sum included unless comm=False."""
+
+    def __init__(self, shell: Shell, k=None, k_q0=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET, diagonal=False,
+                 stored=None):
+        self.shell = shell
+        self.k = None if k is None else np.ascontiguousarray(k, np.float64)
+        self.k_q0 = None if k_q0 is None else np.ascontiguousarray(k_q0, np.float64)
+        if self.k is None and self.k_q0 is None:
+            raise ValueError("need k or k_q0")
+        self.bc_cmb, self.bc_surface = bc_cmb, bc_surface
+        self.diagonal = bool(diagonal)
+        self.stored = None if stored is None else np.ascontiguousarray(stored, np.float64)
+
+    def _struct(self, diagonal=None):
+        s = _OpStruct()
+        s.nl, s.nr = self.shell.nl, self.shell.nr
+        s.coords = self.shell.coords.ctypes.data
+        s.radii = self.shell.radii.ctypes.data
+        s.k = None if self.k is None else self.k.ctypes.data
+        s.k_q0 = None if self.k_q0 is None else self.k_q0.ctypes.data
+        s.bc_cmb, s.bc_surface = self.bc_cmb, self.bc_surface
+        s.diagonal = int(self.diagonal if diagonal is None else diagonal)
+        return s
+
+    def apply(self, src, path="fast", comm=True, diagonal=None):
+        src = [np.ascontiguousarray(src[i], np.float64) for i in range(3)]
+        dst = [np.zeros(self.shell.scalar_shape) for _ in range(3)]
+        s = self._struct(diagonal)
+        if self.stored is not None:
+            lib().tno_epsdivdiv_stored(ctypes.byref(s), _dp(self.stored), _dpp(src), _dpp(dst))
+        elif path == "slow":
+            lib().tno_epsdivdiv_slow(ctypes.byref(s), _dpp(src), _dpp(dst))
+        else:
+            lib().tno_epsdivdiv_fast(ctypes.byref(s), _dpp(src), _dpp(dst))
+        if comm:
+            lib().tno_interface_sum(self.shell.lat_level, self.shell.nr, 3, _dpp(dst))
+        return np.stack(dst)
+
+    def diag(self):
+        """diag(A) via diagonal mode applied to ones (stokes_solver.hpp:390-417)."""
+        return self.apply(np.ones(self.shell.vec_shape), diagonal=True, path="slow" if self.stored is None else "fast")
+
+    def local_matrix(self, d, x, y, r, w):
+        A = np.zeros(324)
+        s = self._struct(False)
+        lib().tno_epsdivdiv_local_matrix(ctypes.byref(s), d, x, y, r, w, _dp(A))
+        return A.reshape(18, 18)
+
+    def vjp_logeta(self, u, lam):
+        """cell gradient of lambda^T A u with respect to log(eta_cell) (Q0 only)."""
+        g = np.zeros(self.shell.cell_shape)
+        s = self._struct(False)
+        uu = [np.ascontiguousarray(u[i]) for i in range(3)]
+        ll = [np.ascontiguousarray(lam[i]) for i in range(3)]
+        rc = lib().tno_epsdivdiv_vjp_logeta(ctypes.byref(s), _dpp(uu), _dpp(ll), _dp(g))
+        if rc != 0:
+            raise ValueError("vjp not supported for this operator")
+        return g
+
+
+def gca_coarsen(fine_op: EpsDivDiv, fine_mats=None):
+    """Two-grid GCA (gca.hpp) of a Neumann fine operator or stored fine matrices."""
+    sh = fine_op.shell
+    nlc, nrc = (sh.nl + 1) // 2, (sh.nr + 1) // 2
+    out = np.zeros((10, nlc - 1, nlc - 1, nrc - 1, 2, 18, 18))
+    s = fine_op._struct(False)
+    fm = None if fine_mats is None else _dp(np.ascontiguousarray(fine_mats))
+    lib().tno_gca_coarsen(ctypes.byref(s), fm, _dp(out))
+    return out
+
+
+class Divergence:
+    """B: velocity (level L) -> pressure (level L-1) (divergence_kerngen.hpp)."""
+
+    def __init__(self, shell: Shell, bc_cmb=DIRICHLET, bc_surface=DIRICHLET):
+        self.shell, self.bc_cmb, self.bc_surface = shell, bc_cmb, bc_surface
+        self.coarse = shell.coarser()
+
+    def _struct(self):
+        s = _OpStruct()
+        s.nl, s.nr = self.shell.nl, self.shell.nr
+        s.coords = self.shell.coords.ctypes.data
+        s.radii = self.shell.radii.ctypes.data
+        s.bc_cmb, s.bc_surface = self.bc_cmb, self.bc_surface
+        return s
+
+    def apply(self, u, comm=True):
+        uu = [np.ascontiguousarray(u[i], np.float64) for i in range(3)]
+        p = np.zeros(self.coarse.scalar_shape)
+        s = self._struct()
+        lib().tno_divergence(ctypes.byref(s), _dpp(uu), _dp(p))
+        if comm:
+            p = self.coarse.interface_sum(p)
+        return p
+
+    def apply_transpose(self, p, comm=True):
+        p = np.ascontiguousarray(p, np.float64)
+        dst = [np.zeros(self.shell.scalar_shape) for _ in range(3)]
+        s = self._struct()
+        lib().tno_gradient(ctypes.byref(s), _dp(p), _dpp(dst))
+        if comm:
+            lib().tno_interface_sum(self.shell.lat_level, self.shell.nr, 3, _dpp(dst))
+        return np.stack(dst)
+
+
+def kmass_lumped(shell: Shell, k):
+    d = np.zeros(shell.scalar_shape)
+    k = np.ascontiguousarray(k, np.float64)
+    lib().tno_kmass_lumped(shell.nl, shell.nr, _dp(shell.coords), _dp(shell.radii), _dp(k), _dp(d))
+    return shell.interface_sum(d)
+
+
+def vector_mass(shell: Shell, v):
+    vv = [np.ascontiguousarray(v[i], np.float64) for i in range(3)]
+    dst = [np.zeros(shell.scalar_shape) for _ in range(3)]
+    lib().tno_vector_mass(shell.nl, shell.nr, _dp(shell.coords), _dp(shell.radii), _dpp(vv), _dpp(dst))
+    lib().tno_interface_sum(shell.lat_level, shell.nr, 3, _dpp(dst))
+    return np.stack(dst)
+
+
+def prolongate_add(fine: Shell, coarse_v, fine_v):
+    """fine_v += P coarse_v (in place), any number of components."""
+    cv = [np.ascontiguousarray(coarse_v[i]) for i in range(coarse_v.shape[0])]
+    fv = [np.ascontiguousarray(fine_v[i]) for i in range(fine_v.shape[0])]
+    lib().tno_prolongate_add(fine.lat_level, fine.rad_level, len(cv), _dpp(cv), _dpp(fv))
+    fine_v[...] = np.stack(fv)
+    return fine_v
+
+
+def restrict(fine: Shell, fine_v):
+    coarse = fine.coarser()
+    fv = [np.ascontiguousarray(fine_v[i]) for i in range(fine_v.shape[0])]
+    cv = [np.zeros(coarse.scalar_shape) for _ in range(len(fv))]
+    lib().tno_restrict(fine.lat_level, fine.rad_level, len(fv), _dpp(fv), _dpp(cv))
+    return np.stack(cv)
+
+
+# --------------------------------------------------------------------------
+# Boundary-condition helpers for right-hand sides
+# --------------------------------------------------------------------------
+def trafo_nt(n):
+    """Rows (n, t1, t2) (local_basis_trafo_normal_tangential.hpp:34-76)."""
+    n = np.asarray(n, np.float64)
+    nn = n / np.linalg.norm(n)
+    a = np.abs(nn)
+    if a[0] <= a[1] and a[0] <= a[2]:
+        ref = np.array([1.0, 0, 0])
+    elif a[1] <= a[0] and a[1] <= a[2]:
+        ref = np.array([0, 1.0, 0])
+    else:
+        ref = np.array([0, 0, 1.0])
+    t1 = np.cross(ref, nn)
+    t1 /= np.linalg.norm(t1)
+    t2 = np.cross(nn, t1)
+    t2 /= np.linalg.norm(t2)
+    return np.stack([nn, t1, t2])
+
+
+def enforce_rhs_bcs(shell: Shell, f, bc_cmb, bc_surface):
+    """Zero Dirichlet rows and the normal component on free-slip boundaries
+    (strong_algebraic_dirichlet_enforcement.hpp:114-123,
+    strong_algebraic_freeslip_enforcement.hpp:22-38)."""
+    f = f.copy()
+    for r, bc in ((0, bc_cmb), (shell.nr - 1, bc_surface)):
+        if bc == DIRICHLET:
+            f[:, :, :, :, r] = 0.0
+        elif bc == FREESLIP:
+            n = shell.coords  # radial direction
+            un = np.einsum("cdxy,dxyc->dxy", f[:, :, :, :, r], n) / np.sum(n * n, axis=-1)
+            f[:, :, :, :, r] -= np.moveaxis(un[..., None] * n, -1, 0)
+    return f
+
+
+# --------------------------------------------------------------------------
+# Solvers (numpy restatements of linalg/solvers/*.hpp)
+# --------------------------------------------------------------------------
+def power_iteration(apply_scaled, start, dot, iterations):
+    """power_iteration.hpp:15-57 with a caller-provided start vector."""
+    it = start.copy()
+    norm = math.sqrt(dot(it, it))
+    if norm < np.finfo(np.float64).tiny:
+        return 1.0
+    it = it / norm
+    aux = apply_scaled(it)
+    radius = 0.0
+    for _ in range(iterations):
+        norm = math.sqrt(dot(aux, aux))
+        if norm < np.finfo(np.float64).tiny:
+            return radius if radius > 0.0 else 1.0
+        it = aux / norm
+        aux = apply_scaled(it)
+        radius = dot(it, aux)
+    return radius
+
+
+@dataclass
+class Chebyshev:
+    """Chebyshev-Jacobi smoother (chebyshev.hpp:102-176)."""
+
+    order: int
+    inv_diag: np.ndarray
+    iterations: int = 1
+    lambda_max_est: float | None = None
+
+    def solve(self, A, x, b):
+        ev = self.lambda_max_est
+        if ev is None or not np.isfinite(ev) or ev <= 0:
+            ev = 1.0
+        lmax, lmin = 1.5 * ev, 0.1 * ev
+        theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+        sigma = theta / delta
+        rho = 1.0 / sigma
+        d = None
+        for _ in range(self.iterations):
+            z = (b - A(x)) * self.inv_diag
+            d = z / theta
+            x = x + d
+            for _i in range(2, self.order + 1):
+                rho_new = 1.0 / (2.0 * sigma - rho)
+                beta = rho_new * rho
+                alpha = 2.0 * rho_new / delta
+                z = (b - A(x)) * self.inv_diag
+                d = alpha * z + beta * d
+                x = x + d
+                rho = rho_new
+        return x
+
+
+def pcg(A, x, b, dot, max_iter, rtol, atol=1e-16, precond=None, history=None):
+    """pcg.hpp:81-169."""
+    r = b - A(x)
+    z = r.copy() if precond is None else precond(r)
+    p = z.copy()
+    init = math.sqrt(dot(r, r))
+    if history is not None:
+        history.append(init)
+    if init < atol:
+        return x
+    for it in range(1, max_iter + 1):
+        an = dot(z, r)
+        ap = A(p)
+        ad = dot(ap, p)
+        if abs(ad) < np.finfo(np.float64).tiny:
+            return x
+        alpha = an / ad
+        x = x + alpha * p
+        r = r - alpha * ap
+        res = math.sqrt(dot(r, r))
+        if history is not None:
+            history.append(res)
+        if res / init <= rtol or res < atol:
+            return x
+        z = r.copy() if precond is None else precond(r)
+        bn = dot(z, r)
+        if abs(an) < np.finfo(np.float64).tiny:
+            return x
+        p = z + (bn / an) * p
+    return x
+
+
+class Multigrid:
+    """V-cycle (multigrid.hpp:216-432); levels[0] is the coarsest."""
+
+    def __init__(self, ops, shells, smoothers, coarse_solve, num_cycles=1):
+        self.ops, self.shells, self.smoothers = ops, shells, smoothers
+        self.coarse_solve, self.num_cycles = coarse_solve, num_cycles
+
+    def _rec(self, level, x, b):
+        if level == 0:
+            return self.coarse_solve(self.ops[0], x, b)
+        A = self.ops[level]
+        x = self.smoothers[level].solve(A, x, b)
+        res = b - A(x)
+        rc = restrict(self.shells[level], res)
+        ec = np.zeros_like(rc)
+        ec = self._rec(level - 1, ec, rc)
+        prolongate_add(self.shells[level], ec, x)
+        x = self.smoothers[level].solve(A, x, b)
+        return x
+
+    def solve(self, x, b):
+        for _ in range(self.num_cycles):
+            x = self._rec(len(self.ops) - 1, x, b)
+        return x
+
+
+def fgmres(A, x, b, dot, precond, restart, rtol, atol, max_iter, history=None):
+    """fgmres.hpp:109-373 (modified Gram-Schmidt, Givens rotations)."""
+    eps = np.finfo(np.float64).eps
+    r = b - A(x)
+    beta0 = math.sqrt(dot(r, r))
+    init = beta0
+    if history is not None:
+        history.append(1.0)
+    if beta0 <= atol:
+        return x, 0
+    total = 0
+    m = restart
+    while total < max_iter:
+        V = [r / beta0]
+        Z = []
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        cs = np.zeros(m + 1)
+        sn = np.zeros(m + 1)
+        g[0] = beta0
+        inner = 0
+        j = 0
+        while j < m and total < max_iter:
+            z = precond(V[j])
+            if not np.all(np.isfinite(z)):
+                z = V[j].copy()
+            Z.append(z)
+            w = A(z)
+            for i in range(j + 1):
+                hij = dot(w, V[i])
+                H[i, j] = hij
+                w = w - hij * V[i]
+            h = math.sqrt(dot(w, w))
+            if h < eps * init:
+                H[j + 1, j] = 0
+                inner = j + 1
+                break
+            H[j + 1, j] = h
+            V.append(w / h)
+            for i in range(j):
+                t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                H[i, j] = t
+            a, bb = H[j, j], H[j + 1, j]
+            rab = math.hypot(a, bb)
+            cs[j] = 1.0 if rab == 0 else a / rab
+            sn[j] = 0.0 if rab == 0 else bb / rab
+            H[j, j] = rab
+            H[j + 1, j] = 0
+            if abs(H[j, j]) < eps:
+                inner = j
+                break
+            gj, gj1 = g[j], g[j + 1]
+            g[j] = cs[j] * gj + sn[j] * gj1
+            g[j + 1] = -sn[j] * gj + cs[j] * gj1
+            abs_res = abs(g[j + 1])
+            if history is not None:
+                history.append(abs_res / init)
+            if not np.isfinite(abs_res):
+                inner = j
+                total += 1
+                break
+            inner = j + 1
+            if abs_res / init <= rtol or abs_res < atol:
+                break
+            j += 1
+            total += 1
+        y = np.zeros(inner)
+        for row in range(inner - 1, -1, -1):
+            s = g[row] - sum(H[row, c] * y[c] for c in range(row + 1, inner))
+            y[row] = s / H[row, row]
+        for i in range(inner):
+            x = x + y[i] * Z[i]
+        r = b - A(x)
+        beta0 = math.sqrt(dot(r, r))
+        if not np.isfinite(beta0):
+            return x, total
+        if beta0 <= atol or beta0 / init <= rtol:
+            return x, total
+    return x, total
+
+
+# --------------------------------------------------------------------------
+# Seeded synthetic inputs (shared definition with the product's generators is
+# NOT assumed: tests create inputs here and hand them to both sides).
+# --------------------------------------------------------------------------
+def seeded_normal(shape, seed):
+    return np.random.default_rng(seed).standard_normal(shape)

@@ -1,0 +1,337 @@
+// extern "C" boundary (include/terra_b200.h). Exceptions never cross it: every
+// entry point converts them into a status code plus a thread-local message.
+#include <cstring>
+#include <string>
+
+#include "../../include/terra_b200.h"
+#include "tn_runtime.hpp"
+
+struct tn_shell {
+    std::unique_ptr<tn::Shell> impl;
+};
+struct tn_operator {
+    tn::EpsDivDivOp op;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f)
+{
+    try {
+        g_last_error.clear();
+        f();
+        return TN_OK;
+    } catch (const tn::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return TN_ERR_ARG;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return TN_ERR_ARG;
+    }
+}
+
+void need(bool cond, const char* msg)
+{
+    if (!cond) throw tn::Error(tn::kErrArg, msg);
+}
+
+int precision_size(int p)
+{
+    if (p == TN_F64) return 8;
+    if (p == TN_F32) return 4;
+    throw tn::Error(tn::kErrArg, "precision must be TN_F64 or TN_F32");
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+const char* tn_last_error(void) { return g_last_error.c_str(); }
+const char* tn_version(void) { return "terra_b200 0.1 (sm_100a)"; }
+
+int tn_shell_create(int lat_level, int rad_level, int num_levels, double r_min, double r_max, tn_shell** out)
+{
+    return guarded([&] {
+        need(out != nullptr, "out is NULL");
+        auto s  = new tn_shell;
+        try {
+            s->impl = tn::make_shell(lat_level, rad_level, num_levels, r_min, r_max);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+void tn_shell_destroy(tn_shell* shell) { delete shell; }
+
+int tn_shell_num_levels(const tn_shell* shell, int* num_levels)
+{
+    return guarded([&] {
+        need(shell && num_levels, "NULL argument");
+        *num_levels = static_cast<int>(shell->impl->levels.size());
+    });
+}
+
+int tn_shell_level_dims(const tn_shell* shell, int level, int* nl, int* nr)
+{
+    return guarded([&] {
+        need(shell && nl && nr, "NULL argument");
+        const auto& L = shell->impl->level(level);
+        *nl           = L.nl();
+        *nr           = L.nr();
+    });
+}
+
+int tn_shell_copy_coords(const tn_shell* shell, int level, double* coords_host)
+{
+    return guarded([&] {
+        need(shell && coords_host, "NULL argument");
+        const auto& h = shell->impl->level(level).host;
+        std::memcpy(coords_host, h.coords.data(), h.coords.size() * sizeof(double));
+    });
+}
+
+int tn_shell_copy_radii(const tn_shell* shell, int level, double* radii_host)
+{
+    return guarded([&] {
+        need(shell && radii_host, "NULL argument");
+        const auto& h = shell->impl->level(level).host;
+        std::memcpy(radii_host, h.radii.data(), h.radii.size() * sizeof(double));
+    });
+}
+
+int tn_shell_copy_ownership(const tn_shell* shell, int level, uint8_t* owned_host)
+{
+    return guarded([&] {
+        need(shell && owned_host, "NULL argument");
+        const auto& h = shell->impl->level(level).host;
+        for (size_t i = 0; i < h.owned_lat.size(); ++i)
+            std::memset(owned_host + i * h.nr, h.owned_lat[i], static_cast<size_t>(h.nr));
+    });
+}
+
+int tn_shell_copy_boundary_mask(const tn_shell* shell, int level, uint8_t* mask_host)
+{
+    return guarded([&] {
+        need(shell && mask_host, "NULL argument");
+        const auto& h = shell->impl->level(level).host;
+        for (size_t i = 0; i < h.owned_lat.size(); ++i)
+            for (int r = 0; r < h.nr; ++r) mask_host[i * h.nr + r] = tn::boundary_flag(r, h.nr);
+    });
+}
+
+int tn_shell_duplicate_classes(const tn_shell* shell, int level, int32_t* class_of_lat_host, int* num_classes)
+{
+    return guarded([&] {
+        need(shell && class_of_lat_host && num_classes, "NULL argument");
+        const auto& h = shell->impl->level(level).host;
+        for (size_t i = 0; i < h.owned_lat.size(); ++i) class_of_lat_host[i] = -1;
+        const int nc = static_cast<int>(h.dup_offset.size()) - 1;
+        for (int c = 0; c < nc; ++c)
+            for (int m = h.dup_offset[c]; m < h.dup_offset[c + 1]; ++m) class_of_lat_host[h.dup_members[m]] = c;
+        *num_classes = nc;
+    });
+}
+
+int tn_mesh_generate_host(int lat_level, int rad_level, double r_min, double r_max, double* coords_host,
+                          double* radii_host, uint8_t* owned_lat_host, int32_t* class_of_lat_host, int* num_classes)
+{
+    return guarded([&] {
+        tn::ShellLevel h;
+        try {
+            h = tn::make_shell_level(lat_level, rad_level, r_min, r_max);
+        } catch (const std::invalid_argument& e) {
+            throw tn::Error(tn::kErrArg, e.what());
+        }
+        if (coords_host) std::memcpy(coords_host, h.coords.data(), h.coords.size() * sizeof(double));
+        if (radii_host) std::memcpy(radii_host, h.radii.data(), h.radii.size() * sizeof(double));
+        if (owned_lat_host) std::memcpy(owned_lat_host, h.owned_lat.data(), h.owned_lat.size());
+        const int nc = static_cast<int>(h.dup_offset.size()) - 1;
+        if (class_of_lat_host) {
+            for (size_t i = 0; i < h.owned_lat.size(); ++i) class_of_lat_host[i] = -1;
+            for (int c = 0; c < nc; ++c)
+                for (int m = h.dup_offset[c]; m < h.dup_offset[c + 1]; ++m) class_of_lat_host[h.dup_members[m]] = c;
+        }
+        if (num_classes) *num_classes = nc;
+    });
+}
+
+int tn_shell_check_device_error(tn_shell* shell, int* code)
+{
+    return guarded([&] {
+        need(shell && code, "NULL argument");
+        tn::cuda_check(cudaDeviceSynchronize(), "synchronize");
+        int v = 0;
+        tn::cuda_check(cudaMemcpy(&v, shell->impl->err.get(), sizeof(int), cudaMemcpyDeviceToHost), "read error");
+        tn::cuda_check(cudaMemset(shell->impl->err.get(), 0, sizeof(int)), "clear error");
+        *code = v;
+    });
+}
+
+int tn_epsdivdiv_create(tn_shell* shell, int level, int precision, const void* k_nodal_dev, const void* k_cell_dev,
+                        int bc_cmb, int bc_surface, int diagonal, tn_operator** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        need((k_nodal_dev == nullptr) != (k_cell_dev == nullptr), "exactly one of k_nodal / k_cell must be given");
+        need(bc_cmb >= 0 && bc_cmb <= 2 && bc_surface >= 0 && bc_surface <= 2, "invalid boundary condition");
+        const int   es = precision_size(precision);
+        const auto& L  = shell->impl->level(level);
+        auto        o  = new tn_operator;
+        try {
+            o->op.shell     = shell->impl.get();
+            o->op.level     = level;
+            o->op.precision = precision;
+            o->op.q0        = k_cell_dev != nullptr;
+            o->op.bc_cmb    = bc_cmb;
+            o->op.bc_surf   = bc_surface;
+            o->op.diagonal  = diagonal != 0;
+            const size_t n  = static_cast<size_t>(o->op.q0 ? L.cells() : L.nodes());
+            o->op.k.alloc(n * es);
+            tn::cuda_check(cudaMemcpy(o->op.k.get(), o->op.q0 ? k_cell_dev : k_nodal_dev, n * es,
+                                      cudaMemcpyDeviceToDevice),
+                           "copy coefficient");
+        } catch (...) {
+            delete o;
+            throw;
+        }
+        *out = o;
+    });
+}
+
+void tn_operator_destroy(tn_operator* op) { delete op; }
+
+int tn_operator_set_modes(tn_operator* op, int apply_mode, int comm_mode)
+{
+    return guarded([&] {
+        need(op, "NULL operator");
+        need(apply_mode == TN_REPLACE || apply_mode == TN_ADD, "invalid apply mode");
+        need(comm_mode == TN_SKIP_COMMUNICATION || comm_mode == TN_COMMUNICATE_ADDITIVELY, "invalid comm mode");
+        op->op.apply_mode = apply_mode;
+        op->op.comm_mode  = comm_mode;
+    });
+}
+
+int tn_operator_set_diagonal(tn_operator* op, int diagonal)
+{
+    return guarded([&] {
+        need(op, "NULL operator");
+        op->op.diagonal = diagonal != 0;
+    });
+}
+
+int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surface)
+{
+    return guarded([&] {
+        need(op, "NULL operator");
+        need(bc_cmb >= 0 && bc_cmb <= 2 && bc_surface >= 0 && bc_surface <= 2, "invalid boundary condition");
+        op->op.bc_cmb  = bc_cmb;
+        op->op.bc_surf = bc_surface;
+    });
+}
+
+int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x)
+{
+    return guarded([&] {
+        need(op, "NULL operator");
+        need(tile_y >= 0 && tile_y <= 7 && chunk_x >= 0 && chunk_x <= 64, "tile out of range");
+        op->op.tile_y  = tile_y;
+        op->op.chunk_x = chunk_x;
+    });
+}
+
+int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* dst_dev, void* stream)
+{
+    return guarded([&] {
+        need(op && src_dev && dst_dev, "NULL argument");
+        for (int c = 0; c < 3; ++c) need(src_dev[c] && dst_dev[c], "NULL component pointer");
+        if (op->op.precision == TN_F64)
+            op->op.apply<double>(reinterpret_cast<const double* const*>(src_dev),
+                                 reinterpret_cast<double* const*>(dst_dev), as_stream(stream));
+        else
+            op->op.apply<float>(reinterpret_cast<const float* const*>(src_dev),
+                                reinterpret_cast<float* const*>(dst_dev), as_stream(stream));
+    });
+}
+
+int tn_interface_sum(tn_shell* shell, int level, int precision, int ncomp, void* const* comps_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell && comps_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        precision_size(precision);
+        const auto& L = shell->impl->level(level);
+        int         rc;
+        if (precision == TN_F64)
+            rc = tn::interface_sum<double>(L.iface, L.nr(), ncomp, reinterpret_cast<double* const*>(comps_dev),
+                                           as_stream(stream));
+        else
+            rc = tn::interface_sum<float>(L.iface, L.nr(), ncomp, reinterpret_cast<float* const*>(comps_dev),
+                                          as_stream(stream));
+        if (rc) throw tn::Error(tn::kErrCuda, "interface sum launch failed");
+    });
+}
+
+int tn_vec_lincomb(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, double c0, int nterms,
+                   const double* c, const void* const* x0_dev, const void* const* x1_dev, const void* const* x2_dev,
+                   void* stream)
+{
+    return guarded([&] {
+        need(shell && y_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4 && nterms >= 0 && nterms <= 3, "bad ncomp / nterms");
+        need(nterms == 0 || c != nullptr, "coefficients missing");
+        precision_size(precision);
+        const auto&   L = shell->impl->level(level);
+        const int64_t n = L.nodes();
+        int           rc;
+        if (precision == TN_F64) {
+            double cc[3] = {nterms > 0 ? c[0] : 0, nterms > 1 ? c[1] : 0, nterms > 2 ? c[2] : 0};
+            rc           = tn::lincomb<double>(n, ncomp, reinterpret_cast<double* const*>(y_dev), c0, nterms, cc,
+                                     reinterpret_cast<const double* const*>(x0_dev),
+                                     reinterpret_cast<const double* const*>(x1_dev),
+                                     reinterpret_cast<const double* const*>(x2_dev), as_stream(stream));
+        } else {
+            float cc[3] = {nterms > 0 ? float(c[0]) : 0.f, nterms > 1 ? float(c[1]) : 0.f, nterms > 2 ? float(c[2]) : 0.f};
+            rc          = tn::lincomb<float>(n, ncomp, reinterpret_cast<float* const*>(y_dev), float(c0), nterms, cc,
+                                    reinterpret_cast<const float* const*>(x0_dev),
+                                    reinterpret_cast<const float* const*>(x1_dev),
+                                    reinterpret_cast<const float* const*>(x2_dev), as_stream(stream));
+        }
+        if (rc) throw tn::Error(tn::kErrCuda, "lincomb launch failed");
+    });
+}
+
+int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev,
+               const void* const* b_dev, double* result, void* stream)
+{
+    return guarded([&] {
+        need(shell && a_dev && b_dev && result, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        precision_size(precision);
+        const auto& L   = shell->impl->level(level);
+        double*     red = shell->impl->red.as<double>();
+        int         rc;
+        if (precision == TN_F64)
+            rc = tn::masked_dot<double>(L.nodes(), L.nr(), ncomp, L.owned_lat.as<uint8_t>(),
+                                        reinterpret_cast<const double* const*>(a_dev),
+                                        reinterpret_cast<const double* const*>(b_dev), red, red + 8, as_stream(stream));
+        else
+            rc = tn::masked_dot<float>(L.nodes(), L.nr(), ncomp, L.owned_lat.as<uint8_t>(),
+                                       reinterpret_cast<const float* const*>(a_dev),
+                                       reinterpret_cast<const float* const*>(b_dev), red, red + 8, as_stream(stream));
+        if (rc) throw tn::Error(tn::kErrCuda, "dot launch failed");
+        tn::cuda_check(cudaMemcpyAsync(result, red, sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)),
+                       "dot readback");
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "dot sync");
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,646 @@
+// epsilon-div-div wedge operator apply for sm_100a (FP64 and FP32).
+//
+// Semantics follow the reference's EpsilonDivDivKerngen (src/terra/fe/wedge/
+// operators/shell/epsilon_divdiv_kerngen.hpp): 1-point centroid quadrature,
+// k_eval = mean of the six nodal coefficients (or a per-cell Q0 value),
+// Dirichlet rows reduced to their diagonal (:1569-1602), free-slip as
+// P A P + diag_nn(A) n n^T on boundary nodes (:1638-2198), and a diagonal mode
+// that applies diag(A) (rotated diagonal on free-slip nodes, :2008-2102).
+//
+// Formulation. The wedge Jacobian factorises as J = M diag(r_mid, r_mid, dr/2)
+// with M = [p1-p0, p2-p0, (p0+p1+p2)/3] built from unit-sphere corners only
+// (kernel_helpers.hpp:179-258). With M^{-T} = [e1 e2 e3] the physical gradient
+// of node (m, side s) is g = alpha L_m + s beta e3, alpha = 1/(2 r_mid),
+// beta = 1/(3 dr), L_1 = e1, L_2 = e2, L_0 = -(e1 + e2). The velocity gradient
+// of a wedge is then G = e1 (x) a + e2 (x) b + e3 (x) D (alpha, beta folded in),
+// the stress sigma = k|det J| (2 sym G - 2/3 tr G I), and the nodal outputs
+// sigma g. About 110 flops per wedge instead of two 3x3 inversions plus the
+// per-node gather/scatter of the reference.
+//
+// Work decomposition (one CTA = a tile of TY node lines in y x a chunk of CX
+// node rows in x x all radial nodes of one diamond):
+//   * lanes run along r (CPL consecutive radial cells per lane): coalesced
+//     access to the r-fastest layout, radial node sums by warp shuffles;
+//   * warp w owns cell strip y = y0 - 1 + w; strip-to-strip sums go through
+//     shared memory, the strip left of the tile is recomputed (halo);
+//   * the CTA sweeps x; the two cell columns that meet at a node row are
+//     consecutive steps, so x sums are carried in registers;
+//   * each new node row (TY + 2 columns x nr values, contiguous in global
+//     memory) is staged by one TMA bulk copy per field into a 3-deep ring,
+//     two rows ahead of use. Every node value is written once by its owner:
+//     no atomics, no zeroing pass.
+// Diamond-edge duplicates hold this diamond's partial sums afterwards; the
+// interface-sum kernel completes them.
+#include "tn_device.cuh"
+#include "tn_kernels.hpp"
+
+#include <algorithm>
+
+namespace tn {
+namespace {
+
+constexpr int kMaxWarps = 8;
+
+template <typename T>
+struct EddArgs {
+    int      nl, nr;
+    const T* coords;
+    const T* radii;
+    const T* k;    // nodal coefficient or nullptr
+    const T* kq0;  // per-cell coefficient or nullptr
+    const T* src[3];
+    T*       dst[3];
+    int      bc_cmb, bc_surf;
+    int      add;
+    int      ty, cx;
+    int*     err;
+};
+
+// Wedge corner map m -> hex corner q, q = dx + 2 dy (kernel_helpers.hpp:291-312).
+__device__ __constant__ int kWedgeCorner[2][3] = {{0, 1, 2}, {3, 2, 1}};
+
+template <typename T>
+__device__ __forceinline__ T tabs(T v)
+{
+    return v < T(0) ? -v : v;
+}
+
+// Lateral geometry of one hex column: for each wedge e1, e2, e3 (columns of
+// M^{-T}) and det(M). M columns: a1 = p1 - p0, a2 = p2 - p0, a3 = (p0+p1+p2)/3.
+template <typename T>
+__device__ void column_geometry(const T* coords, int nl, int d, int x, int y, T* g /*20*/)
+{
+    T p[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const T* c = coords + (node_index(nl, 1, d, x + (q & 1), y + (q >> 1), 0)) * 3;
+        p[q][0]    = c[0];
+        p[q][1]    = c[1];
+        p[q][2]    = c[2];
+    }
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const T* p0 = p[kWedgeCorner[w][0]];
+        const T* p1 = p[kWedgeCorner[w][1]];
+        const T* p2 = p[kWedgeCorner[w][2]];
+        T        a1[3], a2[3], a3[3];
+        for (int i = 0; i < 3; ++i) {
+            a1[i] = p1[i] - p0[i];
+            a2[i] = p2[i] - p0[i];
+            a3[i] = (p0[i] + p1[i] + p2[i]) * (T(1) / T(3));
+        }
+        // rows of M^{-1}: (a2 x a3, a3 x a1, a1 x a2) / det
+        T c23[3] = {a2[1] * a3[2] - a2[2] * a3[1], a2[2] * a3[0] - a2[0] * a3[2], a2[0] * a3[1] - a2[1] * a3[0]};
+        T c31[3] = {a3[1] * a1[2] - a3[2] * a1[1], a3[2] * a1[0] - a3[0] * a1[2], a3[0] * a1[1] - a3[1] * a1[0]};
+        T c12[3] = {a1[1] * a2[2] - a1[2] * a2[1], a1[2] * a2[0] - a1[0] * a2[2], a1[0] * a2[1] - a1[1] * a2[0]};
+        T det    = a1[0] * c23[0] + a1[1] * c23[1] + a1[2] * c23[2];
+        T id     = T(1) / det;
+        T* o     = g + 10 * w;
+        for (int i = 0; i < 3; ++i) {
+            o[i]     = c23[i] * id;
+            o[3 + i] = c31[i] * id;
+            o[6 + i] = c12[i] * id;
+        }
+        o[9] = det;
+    }
+}
+
+// Normal-tangential frame rows (n, t1, t2) of a unit normal
+// (local_basis_trafo_normal_tangential.hpp:34-76).
+template <typename T>
+__device__ void trafo_nt(const T n[3], T R[3][3])
+{
+    T ax = tabs(n[0]), ay = tabs(n[1]), az = tabs(n[2]);
+    T ref[3] = {0, 0, 0};
+    if (ax <= ay && ax <= az)
+        ref[0] = 1;
+    else if (ay <= ax && ay <= az)
+        ref[1] = 1;
+    else
+        ref[2] = 1;
+    T t1[3] = {ref[1] * n[2] - ref[2] * n[1], ref[2] * n[0] - ref[0] * n[2], ref[0] * n[1] - ref[1] * n[0]};
+    T m     = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    for (int i = 0; i < 3; ++i) t1[i] /= m;
+    T t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
+    m       = sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+    for (int i = 0; i < 3; ++i) {
+        t2[i] /= m;
+        R[0][i] = n[i];
+        R[1][i] = t1[i];
+        R[2][i] = t2[i];
+    }
+}
+
+// One hex cell (two wedges). u[q][s][c]: corner q, side s (0 bottom, 1 top).
+// ks[q]: k_bot + k_top (nodal) ; kcell used when Q0. Accumulates into out.
+// bcs[s]: boundary condition of side s of this cell (0: interior/Neumann,
+// 1: Dirichlet, 2: free-slip).
+template <typename T, bool DIAG>
+__device__ __forceinline__ void cell_apply(const T (&u)[4][2][3], const T (&ks)[4], T kcell, bool q0, const T* geo,
+                                           T alpha, T beta, T dfac, const int (&bcs)[2], const T (&nrm)[4][3],
+                                           T (&out)[4][2][3])
+{
+    const bool fs_any = (bcs[0] == 2) || (bcs[1] == 2);
+    T          uin[4][2][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            T v0 = u[q][s][0], v1 = u[q][s][1], v2 = u[q][s][2];
+            if (bcs[s] == 1) {
+                v0 = v1 = v2 = T(0);
+            } else if (bcs[s] == 2) {
+                const T dt = nrm[q][0] * v0 + nrm[q][1] * v1 + nrm[q][2] * v2;
+                v0 -= dt * nrm[q][0];
+                v1 -= dt * nrm[q][1];
+                v2 -= dt * nrm[q][2];
+            }
+            uin[q][s][0] = v0;
+            uin[q][s][1] = v1;
+            uin[q][s][2] = v2;
+        }
+
+    T ann[4][2];
+    if (fs_any) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ann[q][0] = ann[q][1] = T(0);
+    }
+
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const T* gw = geo + 10 * w;
+        const int q0i = kWedgeCorner[w][0], q1i = kWedgeCorner[w][1], q2i = kWedgeCorner[w][2];
+        const T   kv  = q0 ? kcell : (ks[q0i] + ks[q1i] + ks[q2i]);
+        const T   kw  = kv * tabs(gw[9]) * dfac;
+        T         E1[3], E2[3], E3[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            E1[i] = alpha * gw[i];
+            E2[i] = alpha * gw[3 + i];
+            E3[i] = beta * gw[6 + i];
+        }
+        if (!DIAG) {
+            T a[3], b[3], D[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T S0 = uin[q0i][0][c] + uin[q0i][1][c];
+                const T S1 = uin[q1i][0][c] + uin[q1i][1][c];
+                const T S2 = uin[q2i][0][c] + uin[q2i][1][c];
+                a[c]       = S1 - S0;
+                b[c]       = S2 - S0;
+                D[c]       = (uin[q0i][1][c] - uin[q0i][0][c]) + (uin[q1i][1][c] - uin[q1i][0][c]) +
+                       (uin[q2i][1][c] - uin[q2i][0][c]);
+            }
+            // G[i][j] = d_i u_j
+            T G[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) G[i][j] = E1[i] * a[j] + E2[i] * b[j] + E3[i] * D[j];
+            const T div = G[0][0] + G[1][1] + G[2][2];
+            const T k2  = T(2) * kw;
+            const T kd  = kw * (T(2) / T(3)) * div;
+            const T s00 = k2 * G[0][0] - kd, s11 = k2 * G[1][1] - kd, s22 = k2 * G[2][2] - kd;
+            const T s01 = kw * (G[0][1] + G[1][0]), s02 = kw * (G[0][2] + G[2][0]), s12 = kw * (G[1][2] + G[2][1]);
+            T       v1[3], v2[3], wv[3];
+            v1[0] = s00 * E1[0] + s01 * E1[1] + s02 * E1[2];
+            v1[1] = s01 * E1[0] + s11 * E1[1] + s12 * E1[2];
+            v1[2] = s02 * E1[0] + s12 * E1[1] + s22 * E1[2];
+            v2[0] = s00 * E2[0] + s01 * E2[1] + s02 * E2[2];
+            v2[1] = s01 * E2[0] + s11 * E2[1] + s12 * E2[2];
+            v2[2] = s02 * E2[0] + s12 * E2[1] + s22 * E2[2];
+            wv[0] = s00 * E3[0] + s01 * E3[1] + s02 * E3[2];
+            wv[1] = s01 * E3[0] + s11 * E3[1] + s12 * E3[2];
+            wv[2] = s02 * E3[0] + s12 * E3[1] + s22 * E3[2];
+            const bool bot_on = bcs[0] != 1, top_on = bcs[1] != 1;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T v0 = -(v1[c] + v2[c]);
+                if (bot_on) {
+                    out[q0i][0][c] += v0 - wv[c];
+                    out[q1i][0][c] += v1[c] - wv[c];
+                    out[q2i][0][c] += v2[c] - wv[c];
+                }
+                if (top_on) {
+                    out[q0i][1][c] += v0 + wv[c];
+                    out[q1i][1][c] += v1[c] + wv[c];
+                    out[q2i][1][c] += v2[c] + wv[c];
+                }
+            }
+        }
+        // Diagonal terms: all nodes in DIAG mode, Dirichlet-side nodes otherwise;
+        // free-slip normal stiffness Ann on free-slip sides.
+        const bool need_diag = DIAG || bcs[0] == 1 || bcs[1] == 1;
+        if (need_diag || fs_any) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const bool dir_side = bcs[s] == 1;
+                const bool fs_side  = bcs[s] == 2;
+                if (!(DIAG || dir_side || fs_side)) continue;
+                const T sg = s == 0 ? T(-1) : T(1);
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    const int q = kWedgeCorner[w][m];
+                    T         g[3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T L = m == 0 ? -(E1[i] + E2[i]) : (m == 1 ? E1[i] : E2[i]);
+                        g[i]      = L + sg * E3[i];
+                    }
+                    const T gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+                    if (fs_side) {
+                        const T ng = nrm[q][0] * g[0] + nrm[q][1] * g[1] + nrm[q][2] * g[2];
+                        if (!DIAG) {
+                            ann[q][s] += kw * (gg + ng * ng * (T(1) / T(3)));
+                        } else {
+                            T R[3][3];
+                            trafo_nt(nrm[q], R);
+                            T v[3];
+#pragma unroll
+                            for (int a_ = 0; a_ < 3; ++a_) {
+                                const T Rg = R[a_][0] * g[0] + R[a_][1] * g[1] + R[a_][2] * g[2];
+                                const T Rs = R[a_][0] * u[q][s][0] + R[a_][1] * u[q][s][1] + R[a_][2] * u[q][s][2];
+                                v[a_]      = kw * (gg + Rg * Rg * (T(1) / T(3))) * Rs;
+                            }
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) out[q][s][c] += R[0][c] * v[0] + R[1][c] * v[1] + R[2][c] * v[2];
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            out[q][s][c] += kw * u[q][s][c] * (gg + g[c] * g[c] * (T(1) / T(3)));
+                    }
+                }
+            }
+        }
+    }
+
+    if (!DIAG && fs_any) {
+        // test-side projection and normal stiffness: o <- P o + Ann (n.u) n
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            if (bcs[s] != 2) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const T* n  = nrm[q];
+                const T  dt = n[0] * out[q][s][0] + n[1] * out[q][s][1] + n[2] * out[q][s][2];
+                const T  un = n[0] * u[q][s][0] + n[1] * u[q][s][1] + n[2] * u[q][s][2];
+                const T  cr = ann[q][s] * un - dt;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out[q][s][c] += cr * n[c];
+            }
+        }
+    }
+}
+
+template <typename T>
+struct SmemLayout {
+    size_t   bar_off, ring_off, geo_off, xch_off, total;
+    uint32_t rowcap;  // bytes per field per row buffer (16-aligned)
+};
+
+template <typename T, int CPL>
+__host__ __device__ inline SmemLayout<T> edd_smem_layout(int nr, int ty, int cx, int nfields)
+{
+    SmemLayout<T> L;
+    L.bar_off       = 0;
+    L.rowcap        = static_cast<uint32_t>(((static_cast<size_t>(ty + 2) * nr * sizeof(T) + 16) + 15) / 16 * 16);
+    L.ring_off      = 64;
+    L.geo_off       = L.ring_off + static_cast<size_t>(3) * nfields * L.rowcap;
+    L.xch_off       = L.geo_off + static_cast<size_t>(ty + 1) * (cx + 1) * 20 * sizeof(T);
+    L.xch_off       = (L.xch_off + 15) / 16 * 16;
+    L.total         = L.xch_off + static_cast<size_t>(2) * (ty + 1) * 32 * 3 * (CPL + 1) * sizeof(T);
+    return L;
+}
+
+template <typename T, int CPL, bool DIAG>
+__global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nl = A.nl, nr = A.nr;
+    const int ty = A.ty, cx = A.cx;
+    const int lane = threadIdx.x, w = threadIdx.y, nwarps = ty + 1;
+    const int d  = blockIdx.z;
+    const int y0 = blockIdx.x * ty;
+    const int xs = blockIdx.y * cx;
+    const int yc = y0 - 1 + w;  // cell strip of this warp
+    const bool q0 = A.kq0 != nullptr;
+    const int  nfields = q0 ? 3 : 4;
+
+    const SmemLayout<T> L   = edd_smem_layout<T, CPL>(nr, ty, cx, nfields);
+    uint64_t*           bar = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    unsigned char*      ring = smem + L.ring_off;
+    T*                  geo  = reinterpret_cast<T*>(smem + L.geo_off);
+    T*                  xch  = reinterpret_cast<T*>(smem + L.xch_off);
+
+    const int ylo    = max(y0 - 1, 0);
+    const int yhi    = min(y0 + ty, nl - 1);
+    const int ncols  = yhi - ylo + 1;
+    const int nrows  = cx + 2;  // node rows xs-1 .. xs+cx
+    const int nsteps = cx + 1;  // cell columns xs-1 .. xs+cx-1
+    const T*  fields[4] = {A.src[0], A.src[1], A.src[2], A.k};
+
+    // Element offset (0..15 bytes / sizeof(T)) of the first staged element of node row xr.
+    auto row_offset = [&](int xr) -> int {
+        const int64_t  e0 = node_index(nl, nr, d, xr, ylo, 0);
+        const uint64_t a  = reinterpret_cast<uint64_t>(fields[0] + e0);
+        return static_cast<int>((a & 15u) / sizeof(T));
+    };
+    auto issue_row = [&](int i) {
+        const int xr   = xs - 1 + i;
+        const int slot = i % 3;
+        if (xr < 0 || xr >= nl) {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&bar[slot])) : "memory");
+            return;
+        }
+        const int64_t e0    = node_index(nl, nr, d, xr, ylo, 0);
+        uint32_t      total = 0;
+        uint32_t      bytes[4];
+        const T*      srcp[4];
+        for (int f = 0; f < nfields; ++f) {
+            const uint64_t a   = reinterpret_cast<uint64_t>(fields[f] + e0);
+            const uint64_t al  = a & ~uint64_t(15);
+            const uint32_t off = static_cast<uint32_t>(a - al);
+            bytes[f]           = (off + static_cast<uint32_t>(ncols) * nr * sizeof(T) + 15u) & ~15u;
+            srcp[f]            = reinterpret_cast<const T*>(al);
+            total += bytes[f];
+        }
+        mbar_arrive_expect_tx(&bar[slot], total);
+        for (int f = 0; f < nfields; ++f)
+            bulk_copy_g2s(ring + (static_cast<size_t>(slot) * nfields + f) * L.rowcap, srcp[f], bytes[f], &bar[slot]);
+    };
+
+    if (w == 0 && lane == 0) {
+        for (int s = 0; s < 3; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int rows_issued = 0;  // meaningful on the issuing thread only
+    if (w == 0 && lane == 0) {
+        for (int i = 0; i < 3 && i < nrows; ++i) {
+            issue_row(i);
+            ++rows_issued;
+        }
+    }
+
+    // Lateral geometry of this strip's cells for the chunk, one cell per lane.
+    const bool strip_ok = yc >= 0 && yc < nl - 1;
+    for (int i = lane; i < nsteps; i += 32) {
+        const int x = xs - 1 + i;
+        T*        g = geo + (static_cast<size_t>(w) * (cx + 1) + i) * 20;
+        if (strip_ok && x >= 0 && x < nl - 1)
+            column_geometry<T>(A.coords, nl, d, x, yc, g);
+        else
+            for (int v = 0; v < 20; ++v) g[v] = T(0);
+    }
+
+    // Per-lane radial constants.
+    T   alpha[CPL], beta[CPL], dfac[CPL];
+    int cbc[CPL][2];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) {
+        const int c = lane * CPL + j;
+        if (c < nr - 1) {
+            const T r0 = A.radii[c], r1 = A.radii[c + 1];
+            const T rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+            alpha[j]   = T(0.5) / rm;
+            beta[j]    = T(1) / (T(6) * hdr);
+            dfac[j]    = rm * rm * hdr * (q0 ? T(1) : T(1) / T(6));
+        } else {
+            alpha[j] = beta[j] = dfac[j] = T(0);
+        }
+        cbc[j][0] = (c == 0) ? A.bc_cmb : 0;
+        cbc[j][1] = (c == nr - 2) ? A.bc_surf : 0;
+    }
+    const int  lane_top = (nr - 2) / CPL;  // lane holding the top radial node
+    const bool has_fs   = (A.bc_cmb == 2) || (A.bc_surf == 2);
+
+    T xcarry[2][CPL + 1][3];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int j = 0; j <= CPL; ++j)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) xcarry[a][j][c] = T(0);
+
+    __syncwarp();
+
+    bool ok        = true;
+    int  rows_done = 0;  // rows this thread has seen land, in order
+    for (int i = 0; i < nsteps; ++i) {
+        const int x = xs - 1 + i;
+        // rows i and i + 1 must be resident
+        if (ok && i == 0) {
+            ok = mbar_wait_bounded(&bar[0], 0);
+            rows_done += ok ? 1 : 0;
+        }
+        if (ok) {
+            ok = mbar_wait_bounded(&bar[(i + 1) % 3], ((i + 1) / 3) & 1);
+            rows_done += ok ? 1 : 0;
+        }
+        if (!ok) report_error(A.err, kDevMbarrierTimeout);
+        const int offA = (x >= 0 && x < nl) ? row_offset(x) : 0;
+        const int offB = (x + 1 >= 0 && x + 1 < nl) ? row_offset(x + 1) : 0;
+        const T*  rowA = reinterpret_cast<const T*>(ring + static_cast<size_t>(i % 3) * nfields * L.rowcap);
+        const T*  rowB = reinterpret_cast<const T*>(ring + static_cast<size_t>((i + 1) % 3) * nfields * L.rowcap);
+        const bool cell_col_ok = strip_ok && x >= 0 && x < nl - 1;
+        const T*   g           = geo + (static_cast<size_t>(w) * (cx + 1) + i) * 20;
+
+        T nrm[4][3];
+        if (has_fs && cell_col_ok) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const T* c  = A.coords + node_index(nl, 1, d, x + (q & 1), yc + (q >> 1), 0) * 3;
+                const T  in = T(1) / sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+                nrm[q][0]   = c[0] * in;
+                nrm[q][1]   = c[1] * in;
+                nrm[q][2]   = c[2] * in;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) nrm[q][0] = nrm[q][1] = nrm[q][2] = T(0);
+        }
+
+        // Radial sums (node rc = bottom of cell rc + top of cell rc - 1) feed the
+        // x carry and the y exchange as soon as a node is complete.
+        T* slot_w = xch + ((static_cast<size_t>(i & 1) * nwarps + w) * 32 + lane) * 3 * (CPL + 1);
+        T  keep[CPL + 1][3];
+        T  bot0[4][3];
+        T  prevtop[4][3];
+        auto finish_node = [&](int j, const T (&nv)[4][3]) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                keep[j][c]        = nv[0][c] + xcarry[0][j][c];
+                slot_w[j * 3 + c] = nv[2][c] + xcarry[1][j][c];
+                xcarry[0][j][c]   = nv[1][c];
+                xcarry[1][j][c]   = nv[3][c];
+            }
+        };
+
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+            const int rc = lane * CPL + j;
+            T         out[4][2][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) out[q][s][c] = T(0);
+            if (ok && cell_col_ok && rc < nr - 1) {
+                T u[4][2][3], ks[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
+                    const int            off = (q & 1) ? offB : offA;
+                    const int            col = yc + (q >> 1) - ylo;
+                    const int            e   = off + col * nr + rc;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap);
+                        u[q][0][c]  = fr[e];
+                        u[q][1][c]  = fr[e + 1];
+                    }
+                    if (!q0) {
+                        const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap);
+                        ks[q]       = kr[e] + kr[e + 1];
+                    } else {
+                        ks[q] = T(0);
+                    }
+                }
+                const T   kcell  = q0 ? A.kq0[node_index(nl - 1, nr - 1, d, x, yc, rc)] : T(0);
+                const int bcs[2] = {cbc[j][0], cbc[j][1]};
+                cell_apply<T, DIAG>(u, ks, kcell, q0, g, alpha[j], beta[j], dfac[j], bcs, nrm, out);
+            }
+            if (j == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) bot0[q][c] = out[q][0][c];
+            } else {
+                T nv[4][3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nv[q][c] = out[q][0][c] + prevtop[q][c];
+                finish_node(j, nv);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) prevtop[q][c] = out[q][1][c];
+        }
+        {
+            // node lane*CPL: bottom of the first cell + top of the previous lane's last cell;
+            // node nr-1 (lane_top only): top of the last cell.
+            T nv[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const T up = shfl_up(prevtop[q][c], 1);
+                    nv[q][c]   = bot0[q][c] + (lane > 0 ? up : T(0));
+                }
+            finish_node(0, nv);
+            finish_node(CPL, prevtop);
+        }
+        __syncthreads();
+        if (w == 0 && lane == 0 && i + 3 < nrows) {
+            issue_row(i + 3);
+            ++rows_issued;
+        }
+
+        const int yn = yc;  // node line owned by warp w (w >= 1)
+        if (ok && w >= 1 && i >= 1 && x < nl && yn < nl) {
+            const T* slot_p = xch + ((static_cast<size_t>(i & 1) * nwarps + (w - 1)) * 32 + lane) * 3 * (CPL + 1);
+#pragma unroll
+            for (int j = 0; j <= CPL; ++j) {
+                const int rn = (j < CPL) ? lane * CPL + j : nr - 1;
+                const bool own = (j < CPL) ? (rn < nr - 1) : (lane == lane_top);
+                if (!own) continue;
+                const int64_t id = node_index(nl, nr, d, x, yn, rn);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const T v = keep[j][c] + slot_p[j * 3 + c];
+                    if (A.add)
+                        A.dst[c][id] += v;
+                    else
+                        A.dst[c][id] = v;
+                }
+            }
+        }
+    }
+    // After a timeout the issuing thread still waits (bounded) for every bulk
+    // copy it issued, so no copy lands in shared memory after the CTA retires.
+    if (w == 0 && lane == 0) {
+        for (int r = rows_done; r < rows_issued; ++r) (void)mbar_wait_bounded(&bar[r % 3], (r / 3) & 1, 100000000ull);
+    }
+}
+
+template <typename T, int CPL, bool DIAG>
+int launch_cfg(EddArgs<T> a, int nfields, cudaStream_t st)
+{
+    constexpr size_t kSmemLimit = 227 * 1024;
+    SmemLayout<T>    L          = edd_smem_layout<T, CPL>(a.nr, a.ty, a.cx, nfields);
+    while (L.total > kSmemLimit && a.cx > 1) {
+        a.cx = (a.cx + 1) / 2;
+        L    = edd_smem_layout<T, CPL>(a.nr, a.ty, a.cx, nfields);
+    }
+    if (L.total > kSmemLimit) return -5;
+    auto                k = epsdivdiv_kernel<T, CPL, DIAG>;
+    static size_t       configured = 0;
+    if (L.total > configured) {
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total)) !=
+            cudaSuccess)
+            return -1;
+        configured = L.total;
+    }
+    const int nl = a.nl;
+    dim3      grid((nl + a.ty - 1) / a.ty, (nl + a.cx - 1) / a.cx, 10);
+    dim3      block(32, a.ty + 1);
+    k<<<grid, block, L.total, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T>
+int launch(const EddArgs<T>& a, bool diag, cudaStream_t st)
+{
+    const int cells = a.nr - 1;
+    const int nf    = a.kq0 ? 3 : 4;
+    if (cells <= 32) return diag ? launch_cfg<T, 1, true>(a, nf, st) : launch_cfg<T, 1, false>(a, nf, st);
+    if (cells <= 64) return diag ? launch_cfg<T, 2, true>(a, nf, st) : launch_cfg<T, 2, false>(a, nf, st);
+    if (cells <= 128) return diag ? launch_cfg<T, 4, true>(a, nf, st) : launch_cfg<T, 4, false>(a, nf, st);
+    return -3;
+}
+
+}  // namespace
+
+template <typename T>
+int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream)
+{
+    EddArgs<T> a;
+    a.nl     = p.nl;
+    a.nr     = p.nr;
+    a.coords = p.coords;
+    a.radii  = p.radii;
+    a.k      = p.k;
+    a.kq0    = p.kq0;
+    for (int c = 0; c < 3; ++c) {
+        a.src[c] = p.src[c];
+        a.dst[c] = p.dst[c];
+    }
+    a.bc_cmb  = p.bc_cmb;
+    a.bc_surf = p.bc_surf;
+    a.add     = p.add;
+    a.err     = p.err;
+    // tile shape: TY node lines per CTA (TY + 1 warps), CX node rows per x chunk
+    a.ty = p.tile_y > 0 ? p.tile_y : std::min(7, p.nl);
+    a.cx = p.chunk_x > 0 ? p.chunk_x : std::min(16, p.nl);
+    if (a.ty + 1 > kMaxWarps) return -4;
+    return launch<T>(a, p.diagonal, stream);
+}
+
+template int epsdivdiv_apply<double>(const EddLaunch<double>&, cudaStream_t);
+template int epsdivdiv_apply<float>(const EddLaunch<float>&, cudaStream_t);
+
+}  // namespace tn

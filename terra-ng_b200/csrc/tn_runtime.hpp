@@ -1,0 +1,178 @@
+// Host runtime objects behind the C ABI: device buffers, the per-level device
+// mesh, and operator objects.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tn_grid.hpp"
+#include "tn_kernels.hpp"
+
+namespace tn {
+
+// Status codes mirrored from terra_b200.h.
+enum Status : int {
+    kOk            = 0,
+    kErrArg        = -1,
+    kErrCuda       = -2,
+    kErrAlloc      = -3,
+    kErrState      = -4,
+    kErrDevice     = -5,
+    kErrUnsupported = -6,
+    kErrNotConverged = -7,
+};
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void cuda_check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw Error(kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Owning device allocation.
+class DevBuf {
+  public:
+    DevBuf() = default;
+    explicit DevBuf(size_t bytes) { alloc(bytes); }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf&)            = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_)
+    {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            p_   = o.p_;
+            n_   = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    void alloc(size_t bytes)
+    {
+        release();
+        if (bytes == 0) return;
+        // pad to 256 bytes so 16-byte-rounded bulk reads never leave the allocation
+        const size_t padded = (bytes + 255) / 256 * 256;
+        if (cudaMalloc(&p_, padded) != cudaSuccess) {
+            cudaGetLastError();
+            p_ = nullptr;
+            throw Error(kErrAlloc, "cudaMalloc of " + std::to_string(padded) + " bytes failed");
+        }
+        n_ = bytes;
+    }
+    void release()
+    {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    template <typename T>
+    T* as() const
+    {
+        return static_cast<T*>(p_);
+    }
+    void*  get() const { return p_; }
+    size_t size() const { return n_; }
+
+  private:
+    void*  p_ = nullptr;
+    size_t n_ = 0;
+};
+
+template <typename T>
+DevBuf upload(const std::vector<T>& v)
+{
+    DevBuf b(v.size() * sizeof(T));
+    if (!v.empty()) cuda_check(cudaMemcpy(b.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return b;
+}
+
+// One mesh level resident on the device (both precisions of the geometry).
+struct DeviceLevel {
+    ShellLevel host;
+    DevBuf     coords64, coords32;  // (10, nl, nl, 3)
+    DevBuf     radii64, radii32;    // (nr)
+    DevBuf     owned_lat;           // (10, nl, nl) uint8
+    DevBuf     dup_offset, dup_members;
+    IfaceTable iface;
+
+    int     nl() const { return host.nl; }
+    int     nr() const { return host.nr; }
+    int64_t nodes() const { return host.num_stored_nodes(); }
+    int64_t cells() const { return 10ll * (host.nl - 1) * (host.nl - 1) * (host.nr - 1); }
+    template <typename T>
+    const T* coords() const;
+    template <typename T>
+    const T* radii() const;
+};
+template <>
+inline const double* DeviceLevel::coords<double>() const
+{
+    return coords64.as<double>();
+}
+template <>
+inline const float* DeviceLevel::coords<float>() const
+{
+    return coords32.as<float>();
+}
+template <>
+inline const double* DeviceLevel::radii<double>() const
+{
+    return radii64.as<double>();
+}
+template <>
+inline const float* DeviceLevel::radii<float>() const
+{
+    return radii32.as<float>();
+}
+
+struct Shell {
+    std::vector<std::unique_ptr<DeviceLevel>> levels;  // 0 = coarsest
+    DevBuf                                    err;     // device error word
+    DevBuf                                    red;     // reduction scratch (partials + result)
+    double                                    r_min = 0, r_max = 0;
+
+    const DeviceLevel& level(int l) const
+    {
+        if (l < 0 || l >= static_cast<int>(levels.size())) throw Error(kErrArg, "level index out of range");
+        return *levels[l];
+    }
+    int* err_word() const { return err.as<int>(); }
+};
+
+std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, double r_min, double r_max);
+
+// epsilon-div-div operator object (EpsilonDivDivKerngen).
+struct EpsDivDivOp {
+    const Shell* shell = nullptr;
+    int          level = 0;
+    int          precision = 0;  // 0 f64, 1 f32
+    DevBuf       k;               // nodal or cell coefficient in `precision`
+    bool         q0 = false;
+    int          bc_cmb = 1, bc_surf = 1;
+    bool         diagonal = false;
+    int          apply_mode = 0;  // 0 replace, 1 add
+    int          comm_mode  = 1;  // 1 communicate additively
+    int          tile_y = 0, chunk_x = 0;
+
+    const DeviceLevel& lvl() const { return shell->level(level); }
+    // dst = A src (mode Replace) / dst += A src (mode Add); interface sum if comm.
+    template <typename T>
+    void apply(const T* const* src, T* const* dst, cudaStream_t st, bool diag_override = false) const;
+};
+
+}  // namespace tn

@@ -1,0 +1,275 @@
+"""Python mirror of the terra_b200 C ABI (include/terra_b200.h) over ctypes.
+
+The product is the CUDA library ``libterra_b200.so`` built in-tree by
+``build.py``; this module only marshals torch CUDA tensors to its entry points.
+It raises when the library is missing: there is no CPU fallback.
+
+Vectors are torch tensors on the GPU: a nodal scalar ``(10, nl, nl, nr)``, a
+velocity a ``(3, 10, nl, nl, nr)`` tensor (components are passed as three
+pointers, so a list of three tensors works too).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libterra_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "terra_b200.h")
+
+TN_OK = 0
+TN_F64, TN_F32 = 0, 1
+NEUMANN, DIRICHLET, FREESLIP = 0, 1, 2
+REPLACE, ADD = 0, 1
+SKIP_COMMUNICATION, COMMUNICATE_ADDITIVELY = 0, 1
+
+_lib = None
+
+
+class TerraError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"terra_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not found: build it with `python terra-ng_b200/build.py`")
+    L = ctypes.CDLL(path)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    vpp = ctypes.POINTER(ctypes.c_void_p)
+    dp = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "tn_last_error": ([], ctypes.c_char_p),
+        "tn_version": ([], ctypes.c_char_p),
+        "tn_shell_create": ([i, i, i, d, d, ctypes.POINTER(vp)], i),
+        "tn_shell_destroy": ([vp], None),
+        "tn_shell_num_levels": ([vp, ctypes.POINTER(i)], i),
+        "tn_shell_level_dims": ([vp, i, ctypes.POINTER(i), ctypes.POINTER(i)], i),
+        "tn_shell_copy_coords": ([vp, i, vp], i),
+        "tn_shell_copy_radii": ([vp, i, vp], i),
+        "tn_shell_copy_ownership": ([vp, i, vp], i),
+        "tn_shell_copy_boundary_mask": ([vp, i, vp], i),
+        "tn_shell_duplicate_classes": ([vp, i, vp, ctypes.POINTER(i)], i),
+        "tn_mesh_generate_host": ([i, i, d, d, vp, vp, vp, vp, ctypes.POINTER(i)], i),
+        "tn_shell_check_device_error": ([vp, ctypes.POINTER(i)], i),
+        "tn_epsdivdiv_create": ([vp, i, i, vp, vp, i, i, i, ctypes.POINTER(vp)], i),
+        "tn_operator_destroy": ([vp], None),
+        "tn_operator_set_modes": ([vp, i, i], i),
+        "tn_operator_set_diagonal": ([vp, i], i),
+        "tn_operator_set_boundary_conditions": ([vp, i, i], i),
+        "tn_operator_set_tile": ([vp, i, i], i),
+        "tn_operator_apply": ([vp, vpp, vpp, vp], i),
+        "tn_interface_sum": ([vp, i, i, i, vpp, vp], i),
+        "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
+        "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def declared_symbols(header: str = HEADER_PATH):
+    """Names of all functions declared in the public header."""
+    import re
+
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tn_[a-z0-9_]+)\s*\(", text)))
+
+
+def _check(rc):
+    if rc != TN_OK:
+        raise TerraError(rc, load().tn_last_error().decode())
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[int(a.data_ptr()) for a in arrs])
+
+
+def _comps(v):
+    if isinstance(v, (list, tuple)):
+        return list(v)
+    if v.dim() == 5:
+        return [v[c] for c in range(v.shape[0])]
+    return [v]
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _prec(dtype):
+    import torch
+
+    if dtype == torch.float64:
+        return TN_F64
+    if dtype == torch.float32:
+        return TN_F32
+    raise TypeError(f"unsupported dtype {dtype}")
+
+
+class Shell:
+    """Mesh hierarchy on the device (tn_shell_*)."""
+
+    def __init__(self, lat_level: int, rad_level: int | None = None, num_levels: int = 1, r_min=0.55, r_max=1.0):
+        L = load()
+        if rad_level is None:
+            rad_level = lat_level
+        h = ctypes.c_void_p()
+        _check(L.tn_shell_create(lat_level, rad_level, num_levels, r_min, r_max, ctypes.byref(h)))
+        self._h = h
+        self.num_levels = num_levels
+        self.lat_level, self.rad_level = lat_level, rad_level
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tn_shell_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def dims(self, level: int = -1):
+        level = level % self.num_levels
+        nl, nr = ctypes.c_int(), ctypes.c_int()
+        _check(load().tn_shell_level_dims(self._h, level, ctypes.byref(nl), ctypes.byref(nr)))
+        return nl.value, nr.value
+
+    def coords(self, level: int = -1):
+        import numpy as np
+
+        nl, _ = self.dims(level)
+        out = np.zeros((10, nl, nl, 3))
+        _check(load().tn_shell_copy_coords(self._h, level % self.num_levels, out.ctypes.data))
+        return out
+
+    def radii(self, level: int = -1):
+        import numpy as np
+
+        _, nr = self.dims(level)
+        out = np.zeros(nr)
+        _check(load().tn_shell_copy_radii(self._h, level % self.num_levels, out.ctypes.data))
+        return out
+
+    def ownership(self, level: int = -1):
+        import numpy as np
+
+        nl, nr = self.dims(level)
+        out = np.zeros((10, nl, nl, nr), np.uint8)
+        _check(load().tn_shell_copy_ownership(self._h, level % self.num_levels, out.ctypes.data))
+        return out
+
+    def boundary_mask(self, level: int = -1):
+        import numpy as np
+
+        nl, nr = self.dims(level)
+        out = np.zeros((10, nl, nl, nr), np.uint8)
+        _check(load().tn_shell_copy_boundary_mask(self._h, level % self.num_levels, out.ctypes.data))
+        return out
+
+    def duplicate_classes(self, level: int = -1):
+        import numpy as np
+
+        nl, _ = self.dims(level)
+        out = np.zeros((10, nl, nl), np.int32)
+        n = ctypes.c_int()
+        _check(load().tn_shell_duplicate_classes(self._h, level % self.num_levels, out.ctypes.data, ctypes.byref(n)))
+        return out, n.value
+
+    def check_device_error(self):
+        c = ctypes.c_int()
+        _check(load().tn_shell_check_device_error(self._h, ctypes.byref(c)))
+        return c.value
+
+    def interface_sum(self, v, level: int = -1, stream=None):
+        comps = _comps(v)
+        _check(load().tn_interface_sum(self._h, level % self.num_levels, _prec(comps[0].dtype), len(comps),
+                                       _ptrs(comps), _stream(stream)))
+        return v
+
+    def dot(self, a, b, level: int = -1, stream=None):
+        ca, cb = _comps(a), _comps(b)
+        out = ctypes.c_double()
+        _check(load().tn_vec_dot(self._h, level % self.num_levels, _prec(ca[0].dtype), len(ca), _ptrs(ca), _ptrs(cb),
+                                 ctypes.byref(out), _stream(stream)))
+        return out.value
+
+    def lincomb(self, y, c0, coeffs=(), xs=(), level: int = -1, stream=None):
+        cy = _comps(y)
+        n = len(coeffs)
+        cc = (ctypes.c_double * max(n, 1))(*coeffs) if n else None
+        xp = [_ptrs(_comps(x)) for x in xs] + [None] * (3 - n)
+        _check(load().tn_vec_lincomb(self._h, level % self.num_levels, _prec(cy[0].dtype), len(cy), _ptrs(cy),
+                                     float(c0), n, cc, xp[0], xp[1], xp[2], _stream(stream)))
+        return y
+
+
+def mesh_generate_host(lat_level: int, rad_level: int, r_min=0.55, r_max=1.0):
+    """Host-only mesh of one level: (coords, radii, owned_lat, class_of_lat, num_classes)."""
+    import numpy as np
+
+    nl, nr = (1 << lat_level) + 1, (1 << rad_level) + 1
+    coords = np.zeros((10, nl, nl, 3))
+    radii = np.zeros(nr)
+    owned = np.zeros((10, nl, nl), np.uint8)
+    cls = np.zeros((10, nl, nl), np.int32)
+    n = ctypes.c_int()
+    _check(load().tn_mesh_generate_host(lat_level, rad_level, r_min, r_max, coords.ctypes.data, radii.ctypes.data,
+                                        owned.ctypes.data, cls.ctypes.data, ctypes.byref(n)))
+    return coords, radii, owned, cls, n.value
+
+
+class EpsDivDiv:
+    """epsilon-div-div operator (tn_epsdivdiv_* / tn_operator_*)."""
+
+    def __init__(self, shell: Shell, level: int = -1, k=None, k_cell=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET,
+                 diagonal=False):
+        L = load()
+        if (k is None) == (k_cell is None):
+            raise ValueError("give exactly one of k (nodal) or k_cell (Q0)")
+        ref = k if k is not None else k_cell
+        self.shell, self.level = shell, level % shell.num_levels
+        self.dtype = ref.dtype
+        h = ctypes.c_void_p()
+        kp = ctypes.c_void_p(k.data_ptr()) if k is not None else None
+        kc = ctypes.c_void_p(k_cell.data_ptr()) if k_cell is not None else None
+        _check(L.tn_epsdivdiv_create(shell.handle, self.level, _prec(self.dtype), kp, kc, bc_cmb, bc_surface,
+                                     int(diagonal), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tn_operator_destroy(self._h)
+            self._h = None
+
+    def set_modes(self, apply_mode=REPLACE, comm_mode=COMMUNICATE_ADDITIVELY):
+        _check(load().tn_operator_set_modes(self._h, apply_mode, comm_mode))
+
+    def set_diagonal(self, flag: bool):
+        _check(load().tn_operator_set_diagonal(self._h, int(flag)))
+
+    def set_boundary_conditions(self, bc_cmb, bc_surface):
+        _check(load().tn_operator_set_boundary_conditions(self._h, bc_cmb, bc_surface))
+
+    def set_tile(self, tile_y=0, chunk_x=0):
+        _check(load().tn_operator_set_tile(self._h, tile_y, chunk_x))
+
+    def apply(self, src, dst, stream=None):
+        cs, cd = _comps(src), _comps(dst)
+        if len(cs) != 3 or len(cd) != 3:
+            raise ValueError("velocity vectors need three components")
+        _check(load().tn_operator_apply(self._h, _ptrs(cs), _ptrs(cd), _stream(stream)))
+        return dst

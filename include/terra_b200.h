@@ -4,7 +4,10 @@
  * Every entry point is extern "C", takes plain pointers and sizes, and returns
  * an int status (TN_OK == 0, negative on error; tn_last_error() describes the
  * last failure of the calling thread). Array arguments named *_dev are device
- * pointers; they must be 16-byte aligned (cudaMalloc / torch allocations are).
+ * pointers aligned to their element size. Input arrays are staged into shared
+ * memory by bulk copies of whole 16-byte blocks, so the 16-byte-aligned blocks
+ * that contain an input array must be readable device memory (true for any
+ * array inside a cudaMalloc / torch allocation).
  * Operations run asynchronously on the caller's CUDA stream (NULL = legacy
  * default stream) unless documented as synchronous.
  *

@@ -33,6 +33,7 @@
 // interface-sum kernel completes them.
 #include "tn_device.cuh"
 #include "tn_kernels.hpp"
+#include "tn_wedge_math.cuh"
 
 #include <algorithm>
 
@@ -55,243 +56,6 @@ struct EddArgs {
     int      ty, cx;
     int*     err;
 };
-
-// Wedge corner map m -> hex corner q, q = dx + 2 dy (kernel_helpers.hpp:291-312).
-__device__ __constant__ int kWedgeCorner[2][3] = {{0, 1, 2}, {3, 2, 1}};
-
-template <typename T>
-__device__ __forceinline__ T tabs(T v)
-{
-    return v < T(0) ? -v : v;
-}
-
-// Lateral geometry of one hex column: for each wedge e1, e2, e3 (columns of
-// M^{-T}) and det(M). M columns: a1 = p1 - p0, a2 = p2 - p0, a3 = (p0+p1+p2)/3.
-template <typename T>
-__device__ void column_geometry(const T* coords, int nl, int d, int x, int y, T* g /*20*/)
-{
-    T p[4][3];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const T* c = coords + (node_index(nl, 1, d, x + (q & 1), y + (q >> 1), 0)) * 3;
-        p[q][0]    = c[0];
-        p[q][1]    = c[1];
-        p[q][2]    = c[2];
-    }
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-        const T* p0 = p[kWedgeCorner[w][0]];
-        const T* p1 = p[kWedgeCorner[w][1]];
-        const T* p2 = p[kWedgeCorner[w][2]];
-        T        a1[3], a2[3], a3[3];
-        for (int i = 0; i < 3; ++i) {
-            a1[i] = p1[i] - p0[i];
-            a2[i] = p2[i] - p0[i];
-            a3[i] = (p0[i] + p1[i] + p2[i]) * (T(1) / T(3));
-        }
-        // rows of M^{-1}: (a2 x a3, a3 x a1, a1 x a2) / det
-        T c23[3] = {a2[1] * a3[2] - a2[2] * a3[1], a2[2] * a3[0] - a2[0] * a3[2], a2[0] * a3[1] - a2[1] * a3[0]};
-        T c31[3] = {a3[1] * a1[2] - a3[2] * a1[1], a3[2] * a1[0] - a3[0] * a1[2], a3[0] * a1[1] - a3[1] * a1[0]};
-        T c12[3] = {a1[1] * a2[2] - a1[2] * a2[1], a1[2] * a2[0] - a1[0] * a2[2], a1[0] * a2[1] - a1[1] * a2[0]};
-        T det    = a1[0] * c23[0] + a1[1] * c23[1] + a1[2] * c23[2];
-        T id     = T(1) / det;
-        T* o     = g + 10 * w;
-        for (int i = 0; i < 3; ++i) {
-            o[i]     = c23[i] * id;
-            o[3 + i] = c31[i] * id;
-            o[6 + i] = c12[i] * id;
-        }
-        o[9] = det;
-    }
-}
-
-// Normal-tangential frame rows (n, t1, t2) of a unit normal
-// (local_basis_trafo_normal_tangential.hpp:34-76).
-template <typename T>
-__device__ void trafo_nt(const T n[3], T R[3][3])
-{
-    T ax = tabs(n[0]), ay = tabs(n[1]), az = tabs(n[2]);
-    T ref[3] = {0, 0, 0};
-    if (ax <= ay && ax <= az)
-        ref[0] = 1;
-    else if (ay <= ax && ay <= az)
-        ref[1] = 1;
-    else
-        ref[2] = 1;
-    T t1[3] = {ref[1] * n[2] - ref[2] * n[1], ref[2] * n[0] - ref[0] * n[2], ref[0] * n[1] - ref[1] * n[0]};
-    T m     = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
-    for (int i = 0; i < 3; ++i) t1[i] /= m;
-    T t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
-    m       = sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
-    for (int i = 0; i < 3; ++i) {
-        t2[i] /= m;
-        R[0][i] = n[i];
-        R[1][i] = t1[i];
-        R[2][i] = t2[i];
-    }
-}
-
-// One hex cell (two wedges). u[q][s][c]: corner q, side s (0 bottom, 1 top).
-// ks[q]: k_bot + k_top (nodal) ; kcell used when Q0. Accumulates into out.
-// bcs[s]: boundary condition of side s of this cell (0: interior/Neumann,
-// 1: Dirichlet, 2: free-slip).
-template <typename T, bool DIAG>
-__device__ __forceinline__ void cell_apply(const T (&u)[4][2][3], const T (&ks)[4], T kcell, bool q0, const T* geo,
-                                           T alpha, T beta, T dfac, const int (&bcs)[2], const T (&nrm)[4][3],
-                                           T (&out)[4][2][3])
-{
-    const bool fs_any = (bcs[0] == 2) || (bcs[1] == 2);
-    T          uin[4][2][3];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            T v0 = u[q][s][0], v1 = u[q][s][1], v2 = u[q][s][2];
-            if (bcs[s] == 1) {
-                v0 = v1 = v2 = T(0);
-            } else if (bcs[s] == 2) {
-                const T dt = nrm[q][0] * v0 + nrm[q][1] * v1 + nrm[q][2] * v2;
-                v0 -= dt * nrm[q][0];
-                v1 -= dt * nrm[q][1];
-                v2 -= dt * nrm[q][2];
-            }
-            uin[q][s][0] = v0;
-            uin[q][s][1] = v1;
-            uin[q][s][2] = v2;
-        }
-
-    T ann[4][2];
-    if (fs_any) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) ann[q][0] = ann[q][1] = T(0);
-    }
-
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-        const T* gw = geo + 10 * w;
-        const int q0i = kWedgeCorner[w][0], q1i = kWedgeCorner[w][1], q2i = kWedgeCorner[w][2];
-        const T   kv  = q0 ? kcell : (ks[q0i] + ks[q1i] + ks[q2i]);
-        const T   kw  = kv * tabs(gw[9]) * dfac;
-        T         E1[3], E2[3], E3[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            E1[i] = alpha * gw[i];
-            E2[i] = alpha * gw[3 + i];
-            E3[i] = beta * gw[6 + i];
-        }
-        if (!DIAG) {
-            T a[3], b[3], D[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const T S0 = uin[q0i][0][c] + uin[q0i][1][c];
-                const T S1 = uin[q1i][0][c] + uin[q1i][1][c];
-                const T S2 = uin[q2i][0][c] + uin[q2i][1][c];
-                a[c]       = S1 - S0;
-                b[c]       = S2 - S0;
-                D[c]       = (uin[q0i][1][c] - uin[q0i][0][c]) + (uin[q1i][1][c] - uin[q1i][0][c]) +
-                       (uin[q2i][1][c] - uin[q2i][0][c]);
-            }
-            // G[i][j] = d_i u_j
-            T G[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) G[i][j] = E1[i] * a[j] + E2[i] * b[j] + E3[i] * D[j];
-            const T div = G[0][0] + G[1][1] + G[2][2];
-            const T k2  = T(2) * kw;
-            const T kd  = kw * (T(2) / T(3)) * div;
-            const T s00 = k2 * G[0][0] - kd, s11 = k2 * G[1][1] - kd, s22 = k2 * G[2][2] - kd;
-            const T s01 = kw * (G[0][1] + G[1][0]), s02 = kw * (G[0][2] + G[2][0]), s12 = kw * (G[1][2] + G[2][1]);
-            T       v1[3], v2[3], wv[3];
-            v1[0] = s00 * E1[0] + s01 * E1[1] + s02 * E1[2];
-            v1[1] = s01 * E1[0] + s11 * E1[1] + s12 * E1[2];
-            v1[2] = s02 * E1[0] + s12 * E1[1] + s22 * E1[2];
-            v2[0] = s00 * E2[0] + s01 * E2[1] + s02 * E2[2];
-            v2[1] = s01 * E2[0] + s11 * E2[1] + s12 * E2[2];
-            v2[2] = s02 * E2[0] + s12 * E2[1] + s22 * E2[2];
-            wv[0] = s00 * E3[0] + s01 * E3[1] + s02 * E3[2];
-            wv[1] = s01 * E3[0] + s11 * E3[1] + s12 * E3[2];
-            wv[2] = s02 * E3[0] + s12 * E3[1] + s22 * E3[2];
-            const bool bot_on = bcs[0] != 1, top_on = bcs[1] != 1;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const T v0 = -(v1[c] + v2[c]);
-                if (bot_on) {
-                    out[q0i][0][c] += v0 - wv[c];
-                    out[q1i][0][c] += v1[c] - wv[c];
-                    out[q2i][0][c] += v2[c] - wv[c];
-                }
-                if (top_on) {
-                    out[q0i][1][c] += v0 + wv[c];
-                    out[q1i][1][c] += v1[c] + wv[c];
-                    out[q2i][1][c] += v2[c] + wv[c];
-                }
-            }
-        }
-        // Diagonal terms: all nodes in DIAG mode, Dirichlet-side nodes otherwise;
-        // free-slip normal stiffness Ann on free-slip sides.
-        const bool need_diag = DIAG || bcs[0] == 1 || bcs[1] == 1;
-        if (need_diag || fs_any) {
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-                const bool dir_side = bcs[s] == 1;
-                const bool fs_side  = bcs[s] == 2;
-                if (!(DIAG || dir_side || fs_side)) continue;
-                const T sg = s == 0 ? T(-1) : T(1);
-#pragma unroll
-                for (int m = 0; m < 3; ++m) {
-                    const int q = kWedgeCorner[w][m];
-                    T         g[3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const T L = m == 0 ? -(E1[i] + E2[i]) : (m == 1 ? E1[i] : E2[i]);
-                        g[i]      = L + sg * E3[i];
-                    }
-                    const T gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-                    if (fs_side) {
-                        const T ng = nrm[q][0] * g[0] + nrm[q][1] * g[1] + nrm[q][2] * g[2];
-                        if (!DIAG) {
-                            ann[q][s] += kw * (gg + ng * ng * (T(1) / T(3)));
-                        } else {
-                            T R[3][3];
-                            trafo_nt(nrm[q], R);
-                            T v[3];
-#pragma unroll
-                            for (int a_ = 0; a_ < 3; ++a_) {
-                                const T Rg = R[a_][0] * g[0] + R[a_][1] * g[1] + R[a_][2] * g[2];
-                                const T Rs = R[a_][0] * u[q][s][0] + R[a_][1] * u[q][s][1] + R[a_][2] * u[q][s][2];
-                                v[a_]      = kw * (gg + Rg * Rg * (T(1) / T(3))) * Rs;
-                            }
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) out[q][s][c] += R[0][c] * v[0] + R[1][c] * v[1] + R[2][c] * v[2];
-                        }
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            out[q][s][c] += kw * u[q][s][c] * (gg + g[c] * g[c] * (T(1) / T(3)));
-                    }
-                }
-            }
-        }
-    }
-
-    if (!DIAG && fs_any) {
-        // test-side projection and normal stiffness: o <- P o + Ann (n.u) n
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            if (bcs[s] != 2) continue;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const T* n  = nrm[q];
-                const T  dt = n[0] * out[q][s][0] + n[1] * out[q][s][1] + n[2] * out[q][s][2];
-                const T  un = n[0] * u[q][s][0] + n[1] * u[q][s][1] + n[2] * u[q][s][2];
-                const T  cr = ann[q][s] * un - dt;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) out[q][s][c] += cr * n[c];
-            }
-        }
-    }
-}
 
 template <typename T>
 struct SmemLayout {
@@ -340,10 +104,12 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
     const int nsteps = cx + 1;  // cell columns xs-1 .. xs+cx-1
     const T*  fields[4] = {A.src[0], A.src[1], A.src[2], A.k};
 
-    // Element offset (0..15 bytes / sizeof(T)) of the first staged element of node row xr.
-    auto row_offset = [&](int xr) -> int {
+    // Element offset (0..15 bytes / sizeof(T)) of the first staged element of
+    // node row xr in the bulk-copied buffer of field f (each field may sit at a
+    // different alignment).
+    auto row_offset = [&](int f, int xr) -> int {
         const int64_t  e0 = node_index(nl, nr, d, xr, ylo, 0);
-        const uint64_t a  = reinterpret_cast<uint64_t>(fields[0] + e0);
+        const uint64_t a  = reinterpret_cast<uint64_t>(fields[f] + e0);
         return static_cast<int>((a & 15u) / sizeof(T));
     };
     auto issue_row = [&](int i) {
@@ -439,8 +205,12 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
             rows_done += ok ? 1 : 0;
         }
         if (!ok) report_error(A.err, kDevMbarrierTimeout);
-        const int offA = (x >= 0 && x < nl) ? row_offset(x) : 0;
-        const int offB = (x + 1 >= 0 && x + 1 < nl) ? row_offset(x + 1) : 0;
+        int offA[4], offB[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            offA[f] = (f < nfields && x >= 0 && x < nl) ? row_offset(f, x) : 0;
+            offB[f] = (f < nfields && x + 1 >= 0 && x + 1 < nl) ? row_offset(f, x + 1) : 0;
+        }
         const T*  rowA = reinterpret_cast<const T*>(ring + static_cast<size_t>(i % 3) * nfields * L.rowcap);
         const T*  rowB = reinterpret_cast<const T*>(ring + static_cast<size_t>((i + 1) % 3) * nfields * L.rowcap);
         const bool cell_col_ok = strip_ok && x >= 0 && x < nl - 1;
@@ -492,17 +262,16 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
-                    const int            off = (q & 1) ? offB : offA;
-                    const int            col = yc + (q >> 1) - ylo;
-                    const int            e   = off + col * nr + rc;
+                    const int*           off = (q & 1) ? offB : offA;
+                    const int            e   = (yc + (q >> 1) - ylo) * nr + rc;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap);
+                        const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap) + off[c];
                         u[q][0][c]  = fr[e];
                         u[q][1][c]  = fr[e + 1];
                     }
                     if (!q0) {
-                        const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap);
+                        const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap) + off[3];
                         ks[q]       = kr[e] + kr[e + 1];
                     } else {
                         ks[q] = T(0);

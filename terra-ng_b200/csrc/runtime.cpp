@@ -63,8 +63,8 @@ void EpsDivDivOp::apply(const T* const* src, T* const* dst, cudaStream_t st, boo
     for (int c = 0; c < 3; ++c) {
         p.src[c] = src[c];
         p.dst[c] = dst[c];
-        if ((reinterpret_cast<uintptr_t>(src[c]) & 15u) != 0 || (reinterpret_cast<uintptr_t>(dst[c]) & 7u) != 0)
-            throw Error(kErrArg, "vector component pointers must be 16-byte aligned");
+        if ((reinterpret_cast<uintptr_t>(src[c]) % sizeof(T)) != 0 || (reinterpret_cast<uintptr_t>(dst[c]) % sizeof(T)) != 0)
+            throw Error(kErrArg, "vector component pointers must be aligned to the element size");
     }
     p.bc_cmb   = bc_cmb;
     p.bc_surf  = bc_surf;

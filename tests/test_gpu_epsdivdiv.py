@@ -161,3 +161,20 @@ def test_level7_consistency(cuda):
     Au32 = torch.zeros_like(u, dtype=torch.float32)
     op32.apply(u.float(), Au32)
     assert rel_err(Au32.double().cpu().numpy(), Au.cpu().numpy()) < 1e-4
+
+
+@pytest.mark.parametrize("level", [2, 4, 6])
+def test_apply_is_deterministic(cuda, level):
+    """No atomics: repeated applies are bitwise identical."""
+    import torch
+
+    sh, k, u = _setup(level, seed=61)
+    gsh = T.Shell(level)
+    op = T.EpsDivDiv(gsh, k=torch.tensor(k, device=cuda), bc_cmb=1, bc_surface=2)
+    src = torch.tensor(u, device=cuda)
+    first = torch.zeros_like(src)
+    op.apply(src, first)
+    for _ in range(20):
+        again = torch.full_like(src, float("nan"))
+        op.apply(src, again)
+        assert torch.equal(again, first)

@@ -242,7 +242,8 @@ int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x)
 {
     return guarded([&] {
         need(op, "NULL operator");
-        need(tile_y >= 0 && tile_y <= 7 && chunk_x >= 0 && chunk_x <= 64, "tile out of range");
+        need(tile_y >= 0 && tile_y <= (op->op.precision == TN_F64 ? 7 : 11) && chunk_x >= 0 && chunk_x <= 64,
+             "tile out of range");
         op->op.tile_y  = tile_y;
         op->op.chunk_x = chunk_x;
     });

@@ -40,7 +40,18 @@
 namespace tn {
 namespace {
 
-constexpr int kMaxWarps = 8;
+// Warps per CTA (tile_y + 1): FP64 needs up to 255 registers per thread (8
+// warps fill the register file), FP32 fits 12 warps.
+template <typename T>
+struct MaxWarps;
+template <>
+struct MaxWarps<double> {
+    static constexpr int value = 8;
+};
+template <>
+struct MaxWarps<float> {
+    static constexpr int value = 12;
+};
 
 template <typename T>
 struct EddArgs {
@@ -59,7 +70,7 @@ struct EddArgs {
 
 template <typename T>
 struct SmemLayout {
-    size_t   bar_off, ring_off, geo_off, xch_off, total;
+    size_t   bar_off, ring_off, geo_off, nrm_off, bco_off, xch_off, total;
     uint32_t rowcap;  // bytes per field per row buffer (16-aligned)
 };
 
@@ -71,14 +82,16 @@ __host__ __device__ inline SmemLayout<T> edd_smem_layout(int nr, int ty, int cx,
     L.rowcap        = static_cast<uint32_t>(((static_cast<size_t>(ty + 2) * nr * sizeof(T) + 16) + 15) / 16 * 16);
     L.ring_off      = 64;
     L.geo_off       = L.ring_off + static_cast<size_t>(3) * nfields * L.rowcap;
-    L.xch_off       = L.geo_off + static_cast<size_t>(ty + 1) * (cx + 1) * 20 * sizeof(T);
+    L.nrm_off       = L.geo_off + static_cast<size_t>(ty + 1) * (cx + 1) * 20 * sizeof(T);
+    L.bco_off       = L.nrm_off + static_cast<size_t>(ty + 1) * (cx + 1) * 12 * sizeof(T);
+    L.xch_off       = L.bco_off + static_cast<size_t>(ty + 1) * (cx + 1) * 36 * sizeof(T);
     L.xch_off       = (L.xch_off + 15) / 16 * 16;
     L.total         = L.xch_off + static_cast<size_t>(2) * (ty + 1) * 32 * 3 * (CPL + 1) * sizeof(T);
     return L;
 }
 
 template <typename T, int CPL, bool DIAG>
-__global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
+__global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddArgs<T> A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int nl = A.nl, nr = A.nr;
@@ -95,6 +108,8 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
     uint64_t*           bar = reinterpret_cast<uint64_t*>(smem + L.bar_off);
     unsigned char*      ring = smem + L.ring_off;
     T*                  geo  = reinterpret_cast<T*>(smem + L.geo_off);
+    T*                  nrms = reinterpret_cast<T*>(smem + L.nrm_off);
+    T*                  bcof = reinterpret_cast<T*>(smem + L.bco_off);
     T*                  xch  = reinterpret_cast<T*>(smem + L.xch_off);
 
     const int ylo    = max(y0 - 1, 0);
@@ -149,15 +164,35 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
         }
     }
 
-    // Lateral geometry of this strip's cells for the chunk, one cell per lane.
+    // Lateral geometry (and corner normals) of this strip's cells for the
+    // chunk, one cell per lane.
     const bool strip_ok = yc >= 0 && yc < nl - 1;
+    const bool has_fs   = (A.bc_cmb == 2) || (A.bc_surf == 2);
     for (int i = lane; i < nsteps; i += 32) {
-        const int x = xs - 1 + i;
-        T*        g = geo + (static_cast<size_t>(w) * (cx + 1) + i) * 20;
-        if (strip_ok && x >= 0 && x < nl - 1)
+        const int x  = xs - 1 + i;
+        T*        g  = geo + (static_cast<size_t>(w) * (cx + 1) + i) * 20;
+        T*        nv = nrms + (static_cast<size_t>(w) * (cx + 1) + i) * 12;
+        if (strip_ok && x >= 0 && x < nl - 1) {
             column_geometry<T>(A.coords, nl, d, x, yc, g);
-        else
+            if (has_fs)
+                for (int q = 0; q < 4; ++q) {
+                    const T* c  = A.coords + node_index(nl, 1, d, x + (q & 1), yc + (q >> 1), 0) * 3;
+                    const T  in = T(1) / sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+                    for (int k = 0; k < 3; ++k) nv[q * 3 + k] = c[k] * in;
+                }
+            // boundary coefficients of the bottom (CMB) and top (surface) cells
+            for (int side = 0; side < 2; ++side) {
+                const int bc = side == 0 ? A.bc_cmb : A.bc_surf;
+                if (bc != 1 && bc != 2) continue;
+                const int rc = side == 0 ? 0 : nr - 2;
+                const T   r0 = A.radii[rc], r1 = A.radii[rc + 1];
+                const T   rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+                boundary_coefficients<T>(g, T(0.5) / rm, T(1) / (T(6) * hdr), rm * rm * hdr * (q0 ? T(1) : T(1) / T(6)),
+                                         side, bc, nv, bcof + ((static_cast<size_t>(w) * (cx + 1) + i) * 2 + side) * 18);
+            }
+        } else {
             for (int v = 0; v < 20; ++v) g[v] = T(0);
+        }
     }
 
     // Per-lane radial constants.
@@ -178,8 +213,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
         cbc[j][0] = (c == 0) ? A.bc_cmb : 0;
         cbc[j][1] = (c == nr - 2) ? A.bc_surf : 0;
     }
-    const int  lane_top = (nr - 2) / CPL;  // lane holding the top radial node
-    const bool has_fs   = (A.bc_cmb == 2) || (A.bc_surf == 2);
+    const int lane_top = (nr - 2) / CPL;  // lane holding the top radial node
 
     T xcarry[2][CPL + 1][3];
 #pragma unroll
@@ -216,20 +250,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
         const bool cell_col_ok = strip_ok && x >= 0 && x < nl - 1;
         const T*   g           = geo + (static_cast<size_t>(w) * (cx + 1) + i) * 20;
 
-        T nrm[4][3];
-        if (has_fs && cell_col_ok) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const T* c  = A.coords + node_index(nl, 1, d, x + (q & 1), yc + (q >> 1), 0) * 3;
-                const T  in = T(1) / sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-                nrm[q][0]   = c[0] * in;
-                nrm[q][1]   = c[1] * in;
-                nrm[q][2]   = c[2] * in;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) nrm[q][0] = nrm[q][1] = nrm[q][2] = T(0);
-        }
+        const T* nrm_col = nrms + (static_cast<size_t>(w) * (cx + 1) + i) * 12;
 
         // Radial sums (node rc = bottom of cell rc + top of cell rc - 1) feed the
         // x carry and the y exchange as soon as a node is complete.
@@ -251,19 +272,16 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
         for (int j = 0; j < CPL; ++j) {
             const int rc = lane * CPL + j;
             T         out[4][2][3];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) out[q][s][c] = T(0);
             if (ok && cell_col_ok && rc < nr - 1) {
-                T u[4][2][3], ks[4];
+                const int e0 = (yc - ylo) * nr + rc;       // corners dy = 0
+                const int e1 = (yc + 1 - ylo) * nr + rc;   // corners dy = 1
+                T         u[4][2][3], ks[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
                     const int*           off = (q & 1) ? offB : offA;
-                    const int            e   = (yc + (q >> 1) - ylo) * nr + rc;
+                    const int            e   = (q >> 1) ? e1 : e0;
+                    T                    kb, kt;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap) + off[c];
@@ -272,14 +290,59 @@ __global__ void __launch_bounds__(32 * kMaxWarps) epsdivdiv_kernel(EddArgs<T> A)
                     }
                     if (!q0) {
                         const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap) + off[3];
-                        ks[q]       = kr[e] + kr[e + 1];
+                        kb          = kr[e];
+                        kt          = kr[e + 1];
+                        ks[q]       = kb + kt;
                     } else {
                         ks[q] = T(0);
                     }
                 }
-                const T   kcell  = q0 ? A.kq0[node_index(nl - 1, nr - 1, d, x, yc, rc)] : T(0);
-                const int bcs[2] = {cbc[j][0], cbc[j][1]};
-                cell_apply<T, DIAG>(u, ks, kcell, q0, g, alpha[j], beta[j], dfac[j], bcs, nrm, out);
+                const T kcell = q0 ? A.kq0[node_index(nl - 1, nr - 1, d, x, yc, rc)] : T(0);
+                if (DIAG) {
+                    const int bcs[2] = {cbc[j][0], cbc[j][1]};
+                    T         nrm[4][3];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            nrm[q][c] = has_fs ? nrm_col[q * 3 + c] : T(0);
+#pragma unroll
+                            for (int sd = 0; sd < 2; ++sd) out[q][sd][c] = T(0);
+                        }
+                    cell_apply<T, true>(u, ks, kcell, q0, g, alpha[j], beta[j], dfac[j], bcs, nrm, out);
+                } else {
+                    // boundary cells: only lane 0 (CMB, j = 0) and lane_top (surface, last j)
+                    const bool b0 = cbc[j][0] != 0;
+                    const bool b1 = cbc[j][1] != 0;
+                    T          un0[4], un1[4];
+                    if (b0) side_inputs<T>(u, 0, cbc[j][0], nrm_col, un0);
+                    if (b1) side_inputs<T>(u, 1, cbc[j][1], nrm_col, un1);
+                    hex_interior<T>(u, ks, kcell, q0, g, alpha[j], beta[j], dfac[j], out);
+#pragma unroll
+                    for (int side = 0; side < 2; ++side) {
+                        if (!(side == 0 ? b0 : b1)) continue;
+                        T raw[4][3];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
+                            const int*           off = (q & 1) ? offB : offA;
+                            const int            e   = ((q >> 1) ? e1 : e0) + side;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                raw[q][c] = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap)[off[c] + e];
+                        }
+                        side_outputs<T>(out, side, side == 0 ? cbc[j][0] : cbc[j][1], ks, kcell, q0,
+                                        bcof + ((static_cast<size_t>(w) * (cx + 1) + i) * 2 + side) * 18, nrm_col, raw,
+                                        side == 0 ? un0 : un1);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int sd = 0; sd < 2; ++sd)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) out[q][sd][c] = T(0);
             }
             if (j == 0) {
 #pragma unroll
@@ -403,9 +466,9 @@ int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream)
     a.add     = p.add;
     a.err     = p.err;
     // tile shape: TY node lines per CTA (TY + 1 warps), CX node rows per x chunk
-    a.ty = p.tile_y > 0 ? p.tile_y : std::min(7, p.nl);
+    a.ty = p.tile_y > 0 ? p.tile_y : std::min(MaxWarps<T>::value - 1, p.nl);
     a.cx = p.chunk_x > 0 ? p.chunk_x : std::min(16, p.nl);
-    if (a.ty + 1 > kMaxWarps) return -4;
+    if (a.ty + 1 > MaxWarps<T>::value) return -4;
     return launch<T>(a, p.diagonal, stream);
 }
 

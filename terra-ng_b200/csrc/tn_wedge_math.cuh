@@ -60,7 +60,7 @@ __host__ __device__ void column_geometry(const T* coords, int nl, int d, int x, 
             o[3 + i] = c31[i] * id;
             o[6 + i] = c12[i] * id;
         }
-        o[9] = det;
+        o[9] = det < T(0) ? -det : det;
     }
 }
 
@@ -130,7 +130,7 @@ __host__ __device__ __forceinline__ void cell_apply(const T (&u)[4][2][3], const
         const T* gw = geo + 10 * w;
         const int q0i = wedge_corner(w, 0), q1i = wedge_corner(w, 1), q2i = wedge_corner(w, 2);
         const T   kv  = q0 ? kcell : (ks[q0i] + ks[q1i] + ks[q2i]);
-        const T   kw  = kv * tabs(gw[9]) * dfac;
+        const T   kw  = kv * gw[9] * dfac;
         T         E1[3], E2[3], E3[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
@@ -252,5 +252,252 @@ __host__ __device__ __forceinline__ void cell_apply(const T (&u)[4][2][3], const
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Interior hex cell: both wedges, no boundary treatment. out is assigned.
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ __forceinline__ void hex_interior(const T (&u)[4][2][3], const T (&ks)[4], T kcell, bool q0,
+                                                      const T* geo, T alpha, T beta, T dfac, T (&out)[4][2][3])
+{
+    // corner sums and radial differences
+    T S[4][3], Dq[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            S[q][c]  = u[q][0][c] + u[q][1][c];
+            Dq[q][c] = u[q][1][c] - u[q][0][c];
+        }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out[q][s][c] = T(0);
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const T*  gw  = geo + 10 * w;
+        const int q0i = wedge_corner(w, 0), q1i = wedge_corner(w, 1), q2i = wedge_corner(w, 2);
+        const T   kv  = q0 ? kcell : (ks[q0i] + ks[q1i] + ks[q2i]);
+        const T   kw  = kv * gw[9] * dfac;  // gw[9] = |det M|
+        T         E1[3], E2[3], E3[3], a[3], b[3], D[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            E1[i] = alpha * gw[i];
+            E2[i] = alpha * gw[3 + i];
+            E3[i] = beta * gw[6 + i];
+            a[i]  = S[q1i][i] - S[q0i][i];
+            b[i]  = S[q2i][i] - S[q0i][i];
+            D[i]  = Dq[q0i][i] + Dq[q1i][i] + Dq[q2i][i];
+        }
+        // symmetric part of G = E1 (x) a + E2 (x) b + E3 (x) D, G[i][j] = d_i u_j
+        const T g00 = E1[0] * a[0] + E2[0] * b[0] + E3[0] * D[0];
+        const T g11 = E1[1] * a[1] + E2[1] * b[1] + E3[1] * D[1];
+        const T g22 = E1[2] * a[2] + E2[2] * b[2] + E3[2] * D[2];
+        const T h01 = E1[0] * a[1] + E1[1] * a[0] + E2[0] * b[1] + E2[1] * b[0] + E3[0] * D[1] + E3[1] * D[0];
+        const T h02 = E1[0] * a[2] + E1[2] * a[0] + E2[0] * b[2] + E2[2] * b[0] + E3[0] * D[2] + E3[2] * D[0];
+        const T h12 = E1[1] * a[2] + E1[2] * a[1] + E2[1] * b[2] + E2[2] * b[1] + E3[1] * D[2] + E3[2] * D[1];
+        const T k2  = T(2) * kw;
+        const T kd  = kw * (T(2) / T(3)) * (g00 + g11 + g22);
+        const T s00 = k2 * g00 - kd, s11 = k2 * g11 - kd, s22 = k2 * g22 - kd;
+        const T s01 = kw * h01, s02 = kw * h02, s12 = kw * h12;
+        T       v1[3], v2[3], wv[3];
+        v1[0] = s00 * E1[0] + s01 * E1[1] + s02 * E1[2];
+        v1[1] = s01 * E1[0] + s11 * E1[1] + s12 * E1[2];
+        v1[2] = s02 * E1[0] + s12 * E1[1] + s22 * E1[2];
+        v2[0] = s00 * E2[0] + s01 * E2[1] + s02 * E2[2];
+        v2[1] = s01 * E2[0] + s11 * E2[1] + s12 * E2[2];
+        v2[2] = s02 * E2[0] + s12 * E2[1] + s22 * E2[2];
+        wv[0] = s00 * E3[0] + s01 * E3[1] + s02 * E3[2];
+        wv[1] = s01 * E3[0] + s11 * E3[1] + s12 * E3[2];
+        wv[2] = s02 * E3[0] + s12 * E3[1] + s22 * E3[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T v12 = v1[c] + v2[c];
+            out[q0i][0][c] -= v12 + wv[c];
+            out[q0i][1][c] += wv[c] - v12;
+            out[q1i][0][c] += v1[c] - wv[c];
+            out[q1i][1][c] += v1[c] + wv[c];
+            out[q2i][0][c] += v2[c] - wv[c];
+            out[q2i][1][c] += v2[c] + wv[c];
+        }
+    }
+}
+
+// Boundary treatment of a hex cell, split around hex_interior:
+//   boundary_inputs  : Dirichlet side -> 0, free-slip side -> tangential part
+//   boundary_outputs : Dirichlet side -> diagonal rows kw u (|g|^2 + g_c^2/3);
+//                      free-slip side -> P out + Ann (n.u) n
+// (epsilon_divdiv_kerngen.hpp:1569-1602, 1966-2004, 2108-2160). u_raw is the
+// unmodified cell input, nrm the four corner unit normals.
+template <typename T>
+__host__ __device__ __forceinline__ void boundary_inputs(T (&u)[4][2][3], const int (&bcs)[2], const T (&nrm)[4][3])
+{
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        if (bcs[s] == 1) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) u[q][s][0] = u[q][s][1] = u[q][s][2] = T(0);
+        } else if (bcs[s] == 2) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const T dt = nrm[q][0] * u[q][s][0] + nrm[q][1] * u[q][s][1] + nrm[q][2] * u[q][s][2];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) u[q][s][c] -= dt * nrm[q][c];
+            }
+        }
+    }
+}
+
+template <typename T>
+__host__ __device__ __forceinline__ void boundary_outputs(const T (&u)[4][2][3], const T (&ks)[4], T kcell, bool q0,
+                                                          const T* geo, T alpha, T beta, T dfac, const int (&bcs)[2],
+                                                          const T (&nrm)[4][3], T (&out)[4][2][3])
+{
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        if (bcs[s] != 1 && bcs[s] != 2) continue;
+        T acc[4][3], ann[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ann[q] = T(0);
+            acc[q][0] = acc[q][1] = acc[q][2] = T(0);
+        }
+        const T sg = s == 0 ? T(-1) : T(1);
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const T* gw = geo + 10 * w;
+            const T  kv = q0 ? kcell : (ks[wedge_corner(w, 0)] + ks[wedge_corner(w, 1)] + ks[wedge_corner(w, 2)]);
+            const T  kw = kv * gw[9] * dfac;
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const int q = wedge_corner(w, m);
+                T         g[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
+                    g[i]      = alpha * L + sg * beta * gw[6 + i];
+                }
+                const T gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+                if (bcs[s] == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) acc[q][c] += kw * u[q][s][c] * (gg + g[c] * g[c] * (T(1) / T(3)));
+                } else {
+                    const T ng = nrm[q][0] * g[0] + nrm[q][1] * g[1] + nrm[q][2] * g[2];
+                    ann[q] += kw * (gg + ng * ng * (T(1) / T(3)));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (bcs[s] == 1) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out[q][s][c] = acc[q][c];
+            } else {
+                const T* n  = nrm[q];
+                const T  dt = n[0] * out[q][s][0] + n[1] * out[q][s][1] + n[2] * out[q][s][2];
+                const T  un = n[0] * u[q][s][0] + n[1] * u[q][s][1] + n[2] * u[q][s][2];
+                const T  cr = ann[q] * un - dt;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out[q][s][c] += cr * n[c];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-column boundary coefficients of a boundary cell (side s: 0 bottom, 1 top)
+// with radial constants (alpha, beta, dfac) of that cell:
+//   Dirichlet: dc[w][m][c] = |det M_w| dfac (|g|^2 + g_c^2 / 3)      18 values
+//   free-slip: fc[w][m]    = |det M_w| dfac (|g|^2 + (n.g)^2 / 3)    6 values
+// so that at run time the diagonal rows are sum_w kv_w dc u and the normal
+// stiffness Ann_q = sum_w kv_w fc (kv_w = coefficient sum of wedge w).
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ __forceinline__ void boundary_coefficients(const T* geo, T alpha, T beta, T dfac, int side, int bc,
+                                                               const T* nrm /*[4][3]*/, T* out)
+{
+    const T sg = side == 0 ? T(-1) : T(1);
+    for (int w = 0; w < 2; ++w) {
+        const T* gw = geo + 10 * w;
+        const T  df = gw[9] * dfac;
+        for (int m = 0; m < 3; ++m) {
+            T g[3];
+            for (int i = 0; i < 3; ++i) {
+                const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
+                g[i]      = alpha * L + sg * beta * gw[6 + i];
+            }
+            const T gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+            if (bc == 1) {
+                for (int c = 0; c < 3; ++c) out[(w * 3 + m) * 3 + c] = df * (gg + g[c] * g[c] * (T(1) / T(3)));
+            } else {
+                const T* n  = nrm + 3 * wedge_corner(w, m);
+                const T  ng = n[0] * g[0] + n[1] * g[1] + n[2] * g[2];
+                out[w * 3 + m] = df * (gg + ng * ng * (T(1) / T(3)));
+            }
+        }
+    }
+}
+
+// Input side of the boundary treatment for side s of a cell: Dirichlet -> 0,
+// free-slip -> tangential part (un[q] = n.u of the raw value is returned).
+template <typename T>
+__host__ __device__ __forceinline__ void side_inputs(T (&u)[4][2][3], int s, int bc, const T* nrm, T (&un)[4])
+{
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (bc == 1) {
+            un[q]      = T(0);
+            u[q][s][0] = u[q][s][1] = u[q][s][2] = T(0);
+        } else {
+            const T* n = nrm + 3 * q;
+            un[q]      = n[0] * u[q][s][0] + n[1] * u[q][s][1] + n[2] * u[q][s][2];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) u[q][s][c] -= un[q] * n[c];
+        }
+    }
+}
+
+// Output side: Dirichlet rows -> diagonal terms of the raw input uraw (side s
+// values, [q][c]); free-slip -> P out + Ann (n.u) n.
+template <typename T>
+__host__ __device__ __forceinline__ void side_outputs(T (&out)[4][2][3], int s, int bc, const T (&ks)[4], T kcell,
+                                                      bool q0, const T* coef, const T* nrm, const T (&uraw)[4][3],
+                                                      const T (&un)[4])
+{
+    T kv[2];
+#pragma unroll
+    for (int w = 0; w < 2; ++w)
+        kv[w] = q0 ? kcell : (ks[wedge_corner(w, 0)] + ks[wedge_corner(w, 1)] + ks[wedge_corner(w, 2)]);
+    if (bc == 1) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out[q][s][c] = T(0);
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const int q = wedge_corner(w, m);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out[q][s][c] += kv[w] * coef[(w * 3 + m) * 3 + c] * uraw[q][c];
+            }
+    } else {
+        T ann[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) ann[wedge_corner(w, m)] += kv[w] * coef[w * 3 + m];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const T* n  = nrm + 3 * q;
+            const T  dt = n[0] * out[q][s][0] + n[1] * out[q][s][1] + n[2] * out[q][s][2];
+            const T  cr = ann[q] * un[q] - dt;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out[q][s][c] += cr * n[c];
+        }
+    }
+}
 
 }  // namespace tn

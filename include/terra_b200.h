@@ -95,6 +95,21 @@ int tn_shell_check_device_error(tn_shell* shell, int* code);
 int tn_epsdivdiv_create(tn_shell* shell, int level, int precision, const void* k_nodal_dev, const void* k_cell_dev,
                         int bc_cmb, int bc_surface, int diagonal, tn_operator** out);
 void tn_operator_destroy(tn_operator* op);
+/* Coupling blocks of the P1-iso-P2 / P1 pair between velocity_level and the
+ * pressure level velocity_level-1:
+ *   divergence B  (DivergenceKerngen, src/terra/fe/wedge/operators/shell/
+ *                  divergence_kerngen.hpp:125-257): src 3 velocity comps, dst 1 pressure;
+ *   gradient  B^T (GradientKerngen, gradient_kerngen.hpp:125-259): src 1, dst 3;
+ *   Stokes [A B^T; B 0] (EpsDivDivStokes, epsilon_divdiv_stokes.hpp:39-84):
+ *                  src / dst 4 components (u_x, u_y, u_z, p), Replace mode only. */
+int tn_divergence_create(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
+                         tn_operator** out);
+int tn_gradient_create(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
+                       tn_operator** out);
+int tn_stokes_create(tn_shell* shell, int velocity_level, int precision, const void* k_nodal_dev,
+                     const void* k_cell_dev, int bc_cmb, int bc_surface, tn_operator** out);
+/* Number of source / destination component pointers an apply takes. */
+int tn_operator_components(const tn_operator* op, int* src_components, int* dst_components);
 /* set_operator_apply_and_communication_modes (epsilon_divdiv_kerngen.hpp:447-453) */
 int tn_operator_set_modes(tn_operator* op, int apply_mode, int comm_mode);
 /* set_diagonal (epsilon_divdiv_kerngen.hpp:455) */
@@ -104,9 +119,31 @@ int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surf
 /* Override the CTA tile (0 = default); for tuning. */
 int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x);
 /* apply_impl: dst = A src (Replace) or dst += A src (Add); with
- * CommunicateAdditively the interface duplicates are summed afterwards. src
- * and dst are arrays of three device pointers (x, y, z components). */
+ * CommunicateAdditively the interface duplicates of dst are summed afterwards.
+ * src and dst are arrays of device pointers, one per component
+ * (tn_operator_components). */
 int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* dst_dev, void* stream);
+
+/* Lumped k-weighted pressure mass diagonal, 6-point rule, interface-summed
+ * (KMass with set_lumped_diagonal, src/terra/fe/wedge/operators/shell/
+ * kmass.hpp:98-181; used with k = 1/eta as the Schur preconditioner,
+ * apps/mantlecirculation/src/stokes_solver.hpp:559-584). */
+int tn_kmass_lumped_diagonal(tn_shell* shell, int level, int precision, const void* k_dev, void* diag_dev,
+                             void* stream);
+/* dst = M src, vector mass matrix, interface-summed (VectorMass,
+ * src/terra/fe/wedge/operators/shell/vector_mass.hpp:60-150). */
+int tn_vector_mass_apply(tn_shell* shell, int level, int precision, const void* const* src_dev, void* const* dst_dev,
+                         void* stream);
+
+/* ---- multigrid transfers ----------------------------------------------------
+ * fine += P coarse (ProlongationVecConstant in Add mode, src/terra/fe/wedge/
+ * operators/shell/prolongation_constant.hpp:102-192) and coarse = R fine
+ * including the coarse interface sum (RestrictionVecConstant,
+ * restriction_constant.hpp:133-250). fine_level >= 1; ncomp 1..4. */
+int tn_prolongate_add(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* coarse_dev,
+                      void* const* fine_dev, void* stream);
+int tn_restrict(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
+                void* const* coarse_dev, void* stream);
 
 /* ---- nodal-vector kernels (VectorQ1Vec / VectorQ1Scalar, src/terra/linalg/
  * vector_q1.hpp:20-304; kernels/common/grid_operations.hpp) --------------- */

@@ -10,7 +10,7 @@ struct tn_shell {
     std::unique_ptr<tn::Shell> impl;
 };
 struct tn_operator {
-    tn::EpsDivDivOp op;
+    std::unique_ptr<tn::Operator> op;
 };
 
 namespace {
@@ -48,6 +48,55 @@ int precision_size(int p)
 }
 
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+namespace {
+void check_bcs(int bc_cmb, int bc_surface)
+{
+    need(bc_cmb >= 0 && bc_cmb <= 2 && bc_surface >= 0 && bc_surface <= 2, "invalid boundary condition");
+}
+
+void init_edd(tn::EpsDivDivOp& e, tn::Shell* sh, int level, int precision, const void* k_nodal_dev,
+              const void* k_cell_dev, int bc_cmb, int bc_surface, int diagonal)
+{
+    need((k_nodal_dev == nullptr) != (k_cell_dev == nullptr), "exactly one of k_nodal / k_cell must be given");
+    check_bcs(bc_cmb, bc_surface);
+    const int   es = precision_size(precision);
+    const auto& L  = sh->level(level);
+    need(L.nr() >= 3, "the operator needs at least two radial layers");
+    e.shell     = sh;
+    e.level     = level;
+    e.precision = precision;
+    e.q0        = k_cell_dev != nullptr;
+    e.bc_cmb    = bc_cmb;
+    e.bc_surf   = bc_surface;
+    e.diagonal  = diagonal != 0;
+    const size_t n = static_cast<size_t>(e.q0 ? L.cells() : L.nodes());
+    e.k.alloc(n * es);
+    tn::cuda_check(cudaMemcpy(e.k.get(), e.q0 ? k_cell_dev : k_nodal_dev, n * es, cudaMemcpyDeviceToDevice),
+                   "copy coefficient");
+}
+
+template <typename Op>
+void init_coupling(Op& o, tn::Shell* sh, int level, int precision, int bc_cmb, int bc_surface)
+{
+    check_bcs(bc_cmb, bc_surface);
+    precision_size(precision);
+    sh->level(level);
+    need(level >= 1, "the velocity level needs a coarser pressure level below it");
+    o.shell     = sh;
+    o.level     = level;
+    o.precision = precision;
+    o.bc_cmb    = bc_cmb;
+    o.bc_surf   = bc_surface;
+}
+
+tn::EpsDivDivOp* as_edd(tn_operator* op)
+{
+    auto* e = dynamic_cast<tn::EpsDivDivOp*>(op->op.get());
+    if (!e) throw tn::Error(tn::kErrArg, "not an epsilon-div-div operator");
+    return e;
+}
 }  // namespace
 
 extern "C" {
@@ -176,34 +225,60 @@ int tn_shell_check_device_error(tn_shell* shell, int* code)
     });
 }
 
+
 int tn_epsdivdiv_create(tn_shell* shell, int level, int precision, const void* k_nodal_dev, const void* k_cell_dev,
                         int bc_cmb, int bc_surface, int diagonal, tn_operator** out)
 {
     return guarded([&] {
         need(shell && out, "NULL argument");
-        need((k_nodal_dev == nullptr) != (k_cell_dev == nullptr), "exactly one of k_nodal / k_cell must be given");
-        need(bc_cmb >= 0 && bc_cmb <= 2 && bc_surface >= 0 && bc_surface <= 2, "invalid boundary condition");
-        const int   es = precision_size(precision);
-        const auto& L  = shell->impl->level(level);
-        auto        o  = new tn_operator;
-        try {
-            o->op.shell     = shell->impl.get();
-            o->op.level     = level;
-            o->op.precision = precision;
-            o->op.q0        = k_cell_dev != nullptr;
-            o->op.bc_cmb    = bc_cmb;
-            o->op.bc_surf   = bc_surface;
-            o->op.diagonal  = diagonal != 0;
-            const size_t n  = static_cast<size_t>(o->op.q0 ? L.cells() : L.nodes());
-            o->op.k.alloc(n * es);
-            tn::cuda_check(cudaMemcpy(o->op.k.get(), o->op.q0 ? k_cell_dev : k_nodal_dev, n * es,
-                                      cudaMemcpyDeviceToDevice),
-                           "copy coefficient");
-        } catch (...) {
-            delete o;
-            throw;
-        }
-        *out = o;
+        auto e = std::make_unique<tn::EpsDivDivOp>();
+        init_edd(*e, shell->impl.get(), level, precision, k_nodal_dev, k_cell_dev, bc_cmb, bc_surface, diagonal);
+        auto o = new tn_operator;
+        o->op  = std::move(e);
+        *out   = o;
+    });
+}
+
+int tn_divergence_create(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
+                         tn_operator** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        auto b = std::make_unique<tn::DivergenceOp>();
+        init_coupling(*b, shell->impl.get(), velocity_level, precision, bc_cmb, bc_surface);
+        auto o = new tn_operator;
+        o->op  = std::move(b);
+        *out   = o;
+    });
+}
+
+int tn_gradient_create(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
+                       tn_operator** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        auto b = std::make_unique<tn::GradientOp>();
+        init_coupling(*b, shell->impl.get(), velocity_level, precision, bc_cmb, bc_surface);
+        auto o = new tn_operator;
+        o->op  = std::move(b);
+        *out   = o;
+    });
+}
+
+int tn_stokes_create(tn_shell* shell, int velocity_level, int precision, const void* k_nodal_dev,
+                     const void* k_cell_dev, int bc_cmb, int bc_surface, tn_operator** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        auto s  = std::make_unique<tn::StokesOp>();
+        auto sh = shell->impl.get();
+        init_coupling(*s, sh, velocity_level, precision, bc_cmb, bc_surface);
+        init_edd(s->A, sh, velocity_level, precision, k_nodal_dev, k_cell_dev, bc_cmb, bc_surface, 0);
+        init_coupling(s->BT, sh, velocity_level, precision, bc_cmb, bc_surface);
+        init_coupling(s->B, sh, velocity_level, precision, bc_cmb, bc_surface);
+        auto o = new tn_operator;
+        o->op  = std::move(s);
+        *out   = o;
     });
 }
 
@@ -215,8 +290,10 @@ int tn_operator_set_modes(tn_operator* op, int apply_mode, int comm_mode)
         need(op, "NULL operator");
         need(apply_mode == TN_REPLACE || apply_mode == TN_ADD, "invalid apply mode");
         need(comm_mode == TN_SKIP_COMMUNICATION || comm_mode == TN_COMMUNICATE_ADDITIVELY, "invalid comm mode");
-        op->op.apply_mode = apply_mode;
-        op->op.comm_mode  = comm_mode;
+        if (dynamic_cast<tn::StokesOp*>(op->op.get()) && apply_mode != TN_REPLACE)
+            throw tn::Error(tn::kErrUnsupported, "the Stokes block operator applies in Replace mode only");
+        op->op->apply_mode = apply_mode;
+        op->op->comm_mode  = comm_mode;
     });
 }
 
@@ -224,7 +301,7 @@ int tn_operator_set_diagonal(tn_operator* op, int diagonal)
 {
     return guarded([&] {
         need(op, "NULL operator");
-        op->op.diagonal = diagonal != 0;
+        as_edd(op)->diagonal = diagonal != 0;
     });
 }
 
@@ -232,9 +309,13 @@ int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surf
 {
     return guarded([&] {
         need(op, "NULL operator");
-        need(bc_cmb >= 0 && bc_cmb <= 2 && bc_surface >= 0 && bc_surface <= 2, "invalid boundary condition");
-        op->op.bc_cmb  = bc_cmb;
-        op->op.bc_surf = bc_surface;
+        check_bcs(bc_cmb, bc_surface);
+        op->op->bc_cmb  = bc_cmb;
+        op->op->bc_surf = bc_surface;
+        if (auto* s = dynamic_cast<tn::StokesOp*>(op->op.get())) {
+            s->A.bc_cmb = s->B.bc_cmb = s->BT.bc_cmb = bc_cmb;
+            s->A.bc_surf = s->B.bc_surf = s->BT.bc_surf = bc_surface;
+        }
     });
 }
 
@@ -242,10 +323,20 @@ int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x)
 {
     return guarded([&] {
         need(op, "NULL operator");
-        need(tile_y >= 0 && tile_y <= (op->op.precision == TN_F64 ? 7 : 11) && chunk_x >= 0 && chunk_x <= 64,
+        auto* e = as_edd(op);
+        need(tile_y >= 0 && tile_y <= (e->precision == TN_F64 ? 7 : 11) && chunk_x >= 0 && chunk_x <= 64,
              "tile out of range");
-        op->op.tile_y  = tile_y;
-        op->op.chunk_x = chunk_x;
+        e->tile_y  = tile_y;
+        e->chunk_x = chunk_x;
+    });
+}
+
+int tn_operator_components(const tn_operator* op, int* src_components, int* dst_components)
+{
+    return guarded([&] {
+        need(op && src_components && dst_components, "NULL argument");
+        *src_components = op->op->src_components();
+        *dst_components = op->op->dst_components();
     });
 }
 
@@ -253,13 +344,107 @@ int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* 
 {
     return guarded([&] {
         need(op && src_dev && dst_dev, "NULL argument");
-        for (int c = 0; c < 3; ++c) need(src_dev[c] && dst_dev[c], "NULL component pointer");
-        if (op->op.precision == TN_F64)
-            op->op.apply<double>(reinterpret_cast<const double* const*>(src_dev),
-                                 reinterpret_cast<double* const*>(dst_dev), as_stream(stream));
+        for (int c = 0; c < op->op->src_components(); ++c) need(src_dev[c] != nullptr, "NULL source component");
+        for (int c = 0; c < op->op->dst_components(); ++c) need(dst_dev[c] != nullptr, "NULL destination component");
+        op->op->apply(const_cast<void* const*>(src_dev), dst_dev, as_stream(stream));
+    });
+}
+
+int tn_kmass_lumped_diagonal(tn_shell* shell, int level, int precision, const void* k_dev, void* diag_dev,
+                             void* stream)
+{
+    return guarded([&] {
+        need(shell && k_dev && diag_dev, "NULL argument");
+        precision_size(precision);
+        const auto& L  = shell->impl->level(level);
+        auto        st = as_stream(stream);
+        int         rc;
+        if (precision == TN_F64) {
+            double* d = static_cast<double*>(diag_dev);
+            tn::zero_components<double>(L.nodes(), 1, &d, st);
+            rc = tn::kmass_lumped_add<double>(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(),
+                                              static_cast<const double*>(k_dev), d, st);
+            if (!rc) rc = tn::interface_sum<double>(L.iface, L.nr(), 1, &d, st);
+        } else {
+            float* d = static_cast<float*>(diag_dev);
+            tn::zero_components<float>(L.nodes(), 1, &d, st);
+            rc = tn::kmass_lumped_add<float>(L.nl(), L.nr(), L.coords<float>(), L.radii<float>(),
+                                             static_cast<const float*>(k_dev), d, st);
+            if (!rc) rc = tn::interface_sum<float>(L.iface, L.nr(), 1, &d, st);
+        }
+        if (rc) throw tn::Error(tn::kErrCuda, "k-mass launch failed");
+    });
+}
+
+int tn_vector_mass_apply(tn_shell* shell, int level, int precision, const void* const* src_dev, void* const* dst_dev,
+                         void* stream)
+{
+    return guarded([&] {
+        need(shell && src_dev && dst_dev, "NULL argument");
+        precision_size(precision);
+        const auto& L  = shell->impl->level(level);
+        auto        st = as_stream(stream);
+        int         rc;
+        if (precision == TN_F64) {
+            auto d = reinterpret_cast<double* const*>(dst_dev);
+            tn::zero_components<double>(L.nodes(), 3, d, st);
+            rc = tn::vector_mass_add<double>(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(),
+                                             reinterpret_cast<const double* const*>(src_dev), d, st);
+            if (!rc) rc = tn::interface_sum<double>(L.iface, L.nr(), 3, d, st);
+        } else {
+            auto d = reinterpret_cast<float* const*>(dst_dev);
+            tn::zero_components<float>(L.nodes(), 3, d, st);
+            rc = tn::vector_mass_add<float>(L.nl(), L.nr(), L.coords<float>(), L.radii<float>(),
+                                            reinterpret_cast<const float* const*>(src_dev), d, st);
+            if (!rc) rc = tn::interface_sum<float>(L.iface, L.nr(), 3, d, st);
+        }
+        if (rc) throw tn::Error(tn::kErrCuda, "vector mass launch failed");
+    });
+}
+
+int tn_prolongate_add(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* coarse_dev,
+                      void* const* fine_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell && coarse_dev && fine_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        need(fine_level >= 1, "fine level needs a coarser level");
+        precision_size(precision);
+        const auto& L = shell->impl->level(fine_level);
+        int         rc;
+        if (precision == TN_F64)
+            rc = tn::prolongate_add<double>(L.nl(), L.nr(), ncomp, reinterpret_cast<const double* const*>(coarse_dev),
+                                            reinterpret_cast<double* const*>(fine_dev), as_stream(stream));
         else
-            op->op.apply<float>(reinterpret_cast<const float* const*>(src_dev),
-                                reinterpret_cast<float* const*>(dst_dev), as_stream(stream));
+            rc = tn::prolongate_add<float>(L.nl(), L.nr(), ncomp, reinterpret_cast<const float* const*>(coarse_dev),
+                                           reinterpret_cast<float* const*>(fine_dev), as_stream(stream));
+        if (rc) throw tn::Error(tn::kErrCuda, "prolongation launch failed");
+    });
+}
+
+int tn_restrict(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
+                void* const* coarse_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell && coarse_dev && fine_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        need(fine_level >= 1, "fine level needs a coarser level");
+        precision_size(precision);
+        const auto& L  = shell->impl->level(fine_level);
+        const auto& Lc = shell->impl->level(fine_level - 1);
+        int         rc;
+        if (precision == TN_F64) {
+            auto c = reinterpret_cast<double* const*>(coarse_dev);
+            rc     = tn::restrict_owned<double>(L.nl(), L.nr(), ncomp, L.owned_lat.as<uint8_t>(),
+                                            reinterpret_cast<const double* const*>(fine_dev), c, as_stream(stream));
+            if (!rc) rc = tn::interface_sum<double>(Lc.iface, Lc.nr(), ncomp, c, as_stream(stream));
+        } else {
+            auto c = reinterpret_cast<float* const*>(coarse_dev);
+            rc     = tn::restrict_owned<float>(L.nl(), L.nr(), ncomp, L.owned_lat.as<uint8_t>(),
+                                           reinterpret_cast<const float* const*>(fine_dev), c, as_stream(stream));
+            if (!rc) rc = tn::interface_sum<float>(Lc.iface, Lc.nr(), ncomp, c, as_stream(stream));
+        }
+        if (rc) throw tn::Error(tn::kErrCuda, "restriction launch failed");
     });
 }
 

@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
     int cbc[CPL][2];
 #pragma unroll
     for (int j = 0; j < CPL; ++j) {
-        const int c = lane * CPL + j;
+        const int c = lane + 32 * j;
         if (c < nr - 1) {
             const T r0 = A.radii[c], r1 = A.radii[c + 1];
             const T rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
@@ -213,7 +213,11 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
         cbc[j][0] = (c == 0) ? A.bc_cmb : 0;
         cbc[j][1] = (c == nr - 2) ? A.bc_surf : 0;
     }
-    const int lane_top = (nr - 2) / CPL;  // lane holding the top radial node
+    // Radial mapping: lane l holds cells l + 32 j (j < CPL), so shared-memory
+    // reads and global stores are consecutive across lanes. The top node nr-1
+    // is the extra node of the lane/iteration holding cell nr-2.
+    const int lane_top = (nr - 2) % 32;
+    const int j_top    = (nr - 2) / 32;
 
     T xcarry[2][CPL + 1][3];
 #pragma unroll
@@ -254,23 +258,22 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 
         // Radial sums (node rc = bottom of cell rc + top of cell rc - 1) feed the
         // x carry and the y exchange as soon as a node is complete.
-        T* slot_w = xch + ((static_cast<size_t>(i & 1) * nwarps + w) * 32 + lane) * 3 * (CPL + 1);
+        T* slot_w = xch + (static_cast<size_t>(i & 1) * nwarps + w) * 3 * (CPL + 1) * 32 + lane;
         T  keep[CPL + 1][3];
-        T  bot0[4][3];
-        T  prevtop[4][3];
+        T  carry31[4][3];  // top of cell 32 j - 1 (lane 31, previous j)
         auto finish_node = [&](int j, const T (&nv)[4][3]) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                keep[j][c]        = nv[0][c] + xcarry[0][j][c];
-                slot_w[j * 3 + c] = nv[2][c] + xcarry[1][j][c];
-                xcarry[0][j][c]   = nv[1][c];
-                xcarry[1][j][c]   = nv[3][c];
+                keep[j][c]                = nv[0][c] + xcarry[0][j][c];
+                slot_w[(j * 3 + c) * 32] = nv[2][c] + xcarry[1][j][c];
+                xcarry[0][j][c]           = nv[1][c];
+                xcarry[1][j][c]           = nv[3][c];
             }
         };
 
 #pragma unroll
         for (int j = 0; j < CPL; ++j) {
-            const int rc = lane * CPL + j;
+            const int rc = lane + 32 * j;
             T         out[4][2][3];
             if (ok && cell_col_ok && rc < nr - 1) {
                 const int e0 = (yc - ylo) * nr + rc;       // corners dy = 0
@@ -344,37 +347,26 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 #pragma unroll
                         for (int c = 0; c < 3; ++c) out[q][sd][c] = T(0);
             }
-            if (j == 0) {
+            {
+                T nv[4][3], top[4][3];
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) bot0[q][c] = out[q][0][c];
-            } else {
-                T nv[4][3];
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) nv[q][c] = out[q][0][c] + prevtop[q][c];
+                    for (int c = 0; c < 3; ++c) {
+                        top[q][c]      = out[q][1][c];
+                        const T up     = shfl_up(top[q][c], 1);
+                        const T below  = lane > 0 ? up : (j > 0 ? carry31[q][c] : T(0));
+                        nv[q][c]       = out[q][0][c] + below;
+                    }
                 finish_node(j, nv);
-            }
+                if (j == j_top) finish_node(CPL, top);
+                if (j + 1 < CPL) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+                    for (int q = 0; q < 4; ++q)
 #pragma unroll
-                for (int c = 0; c < 3; ++c) prevtop[q][c] = out[q][1][c];
-        }
-        {
-            // node lane*CPL: bottom of the first cell + top of the previous lane's last cell;
-            // node nr-1 (lane_top only): top of the last cell.
-            T nv[4][3];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const T up = shfl_up(prevtop[q][c], 1);
-                    nv[q][c]   = bot0[q][c] + (lane > 0 ? up : T(0));
+                        for (int c = 0; c < 3; ++c) carry31[q][c] = __shfl_sync(0xffffffffu, top[q][c], 31);
                 }
-            finish_node(0, nv);
-            finish_node(CPL, prevtop);
+            }
         }
         __syncthreads();
         if (w == 0 && lane == 0 && i + 3 < nrows) {
@@ -384,16 +376,16 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 
         const int yn = yc;  // node line owned by warp w (w >= 1)
         if (ok && w >= 1 && i >= 1 && x < nl && yn < nl) {
-            const T* slot_p = xch + ((static_cast<size_t>(i & 1) * nwarps + (w - 1)) * 32 + lane) * 3 * (CPL + 1);
+            const T* slot_p = xch + (static_cast<size_t>(i & 1) * nwarps + (w - 1)) * 3 * (CPL + 1) * 32 + lane;
 #pragma unroll
             for (int j = 0; j <= CPL; ++j) {
-                const int rn = (j < CPL) ? lane * CPL + j : nr - 1;
+                const int rn = (j < CPL) ? lane + 32 * j : nr - 1;
                 const bool own = (j < CPL) ? (rn < nr - 1) : (lane == lane_top);
                 if (!own) continue;
                 const int64_t id = node_index(nl, nr, d, x, yn, rn);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const T v = keep[j][c] + slot_p[j * 3 + c];
+                    const T v = keep[j][c] + slot_p[(j * 3 + c) * 32];
                     if (A.add)
                         A.dst[c][id] += v;
                     else
@@ -467,7 +459,28 @@ int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream)
     a.err     = p.err;
     // tile shape: TY node lines per CTA (TY + 1 warps), CX node rows per x chunk
     a.ty = p.tile_y > 0 ? p.tile_y : std::min(MaxWarps<T>::value - 1, p.nl);
-    a.cx = p.chunk_x > 0 ? p.chunk_x : std::min(16, p.nl);
+    if (p.chunk_x > 0) {
+        a.cx = p.chunk_x;
+    } else {
+        // One CTA per SM: pick the x-chunk that minimises waves x steps per CTA.
+        static int sms = 0;
+        if (sms == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        }
+        const int ytiles = (p.nl + a.ty - 1) / a.ty;
+        long      best   = -1;
+        for (int cx = 4; cx <= std::max(4, p.nl); ++cx) {
+            const long ctas  = 10L * ytiles * ((p.nl + cx - 1) / cx);
+            const long waves = (ctas + sms - 1) / sms;
+            const long cost  = waves * (cx + 1);
+            if (best < 0 || cost < best || (cost == best && cx > a.cx)) {
+                best = cost;
+                a.cx = cx;
+            }
+        }
+    }
     if (a.ty + 1 > MaxWarps<T>::value) return -4;
     return launch<T>(a, p.diagonal, stream);
 }

@@ -48,7 +48,29 @@ std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, 
 }
 
 template <typename T>
-void EpsDivDivOp::apply(const T* const* src, T* const* dst, cudaStream_t st, bool diag_override) const
+void zero_components(int64_t n, int ncomp, T* const* v, cudaStream_t st)
+{
+    for (int c = 0; c < ncomp; ++c) cuda_check(cudaMemsetAsync(v[c], 0, static_cast<size_t>(n) * sizeof(T), st), "zero");
+}
+template void zero_components<double>(int64_t, int, double* const*, cudaStream_t);
+template void zero_components<float>(int64_t, int, float* const*, cudaStream_t);
+
+namespace {
+template <typename T>
+void check_aligned(const void* p)
+{
+    if (reinterpret_cast<uintptr_t>(p) % sizeof(T) != 0)
+        throw Error(kErrArg, "vector component pointers must be aligned to the element size");
+}
+template <typename T>
+void iface(const DeviceLevel& L, int ncomp, T* const* v, cudaStream_t st)
+{
+    if (interface_sum<T>(L.iface, L.nr(), ncomp, v, st) != 0) throw Error(kErrCuda, "interface sum launch failed");
+}
+}  // namespace
+
+template <typename T>
+void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st) const
 {
     const DeviceLevel& L = lvl();
     EddLaunch<T>       p;
@@ -63,25 +85,103 @@ void EpsDivDivOp::apply(const T* const* src, T* const* dst, cudaStream_t st, boo
     for (int c = 0; c < 3; ++c) {
         p.src[c] = src[c];
         p.dst[c] = dst[c];
-        if ((reinterpret_cast<uintptr_t>(src[c]) % sizeof(T)) != 0 || (reinterpret_cast<uintptr_t>(dst[c]) % sizeof(T)) != 0)
-            throw Error(kErrArg, "vector component pointers must be aligned to the element size");
+        check_aligned<T>(src[c]);
+        check_aligned<T>(dst[c]);
     }
     p.bc_cmb   = bc_cmb;
     p.bc_surf  = bc_surf;
-    p.diagonal = diagonal || diag_override;
+    p.diagonal = diagonal;
     p.add      = apply_mode;
     p.tile_y   = tile_y;
     p.chunk_x  = chunk_x;
     p.err      = shell->err_word();
     const int rc = epsdivdiv_apply<T>(p, st);
     if (rc != 0) throw Error(kErrCuda, "epsdivdiv launch failed (" + std::to_string(rc) + ")");
-    if (comm_mode == 1) {
-        T* comps[3] = {dst[0], dst[1], dst[2]};
-        if (interface_sum<T>(L.iface, L.nr(), 3, comps, st) != 0) throw Error(kErrCuda, "interface sum launch failed");
-    }
+    if (comm_mode == 1) iface<T>(L, 3, dst, st);
 }
 
-template void EpsDivDivOp::apply<double>(const double* const*, double* const*, cudaStream_t, bool) const;
-template void EpsDivDivOp::apply<float>(const float* const*, float* const*, cudaStream_t, bool) const;
+void EpsDivDivOp::apply(void* const* src, void* const* dst, cudaStream_t st)
+{
+    if (precision == 0)
+        apply_t<double>(reinterpret_cast<const double* const*>(src), reinterpret_cast<double* const*>(dst), st);
+    else
+        apply_t<float>(reinterpret_cast<const float* const*>(src), reinterpret_cast<float* const*>(dst), st);
+}
+
+template <typename T>
+void DivergenceOp::apply_t(const T* const* src, T* p, cudaStream_t st) const
+{
+    const DeviceLevel& L = lvl();
+    if (level < 1) throw Error(kErrArg, "divergence needs a coarser pressure level");
+    const DeviceLevel& Lc = shell->level(level - 1);
+    if (apply_mode == 0) zero_components<T>(Lc.nodes(), 1, &p, st);
+    CouplingLaunch<T> c;
+    c.nl     = L.nl();
+    c.nr     = L.nr();
+    c.coords = L.coords<T>();
+    c.radii  = L.radii<T>();
+    c.bc_cmb = bc_cmb;
+    c.bc_surf = bc_surf;
+    for (int k = 0; k < 3; ++k) c.u[k] = src[k];
+    c.p_out = p;
+    if (divergence_apply<T>(c, st) != 0) throw Error(kErrCuda, "divergence launch failed");
+    if (comm_mode == 1) iface<T>(Lc, 1, &p, st);
+}
+
+void DivergenceOp::apply(void* const* src, void* const* dst, cudaStream_t st)
+{
+    if (precision == 0)
+        apply_t<double>(reinterpret_cast<const double* const*>(src), static_cast<double*>(dst[0]), st);
+    else
+        apply_t<float>(reinterpret_cast<const float* const*>(src), static_cast<float*>(dst[0]), st);
+}
+
+template <typename T>
+void GradientOp::apply_t(const T* p, T* const* dst, cudaStream_t st) const
+{
+    const DeviceLevel& L = lvl();
+    if (level < 1) throw Error(kErrArg, "gradient needs a coarser pressure level");
+    if (apply_mode == 0) zero_components<T>(L.nodes(), 3, dst, st);
+    CouplingLaunch<T> c;
+    c.nl      = L.nl();
+    c.nr      = L.nr();
+    c.coords  = L.coords<T>();
+    c.radii   = L.radii<T>();
+    c.bc_cmb  = bc_cmb;
+    c.bc_surf = bc_surf;
+    c.p_in    = p;
+    for (int k = 0; k < 3; ++k) c.u_out[k] = dst[k];
+    if (gradient_apply<T>(c, st) != 0) throw Error(kErrCuda, "gradient launch failed");
+    if (comm_mode == 1) iface<T>(L, 3, dst, st);
+}
+
+void GradientOp::apply(void* const* src, void* const* dst, cudaStream_t st)
+{
+    if (precision == 0)
+        apply_t<double>(static_cast<const double*>(src[0]), reinterpret_cast<double* const*>(dst), st);
+    else
+        apply_t<float>(static_cast<const float*>(src[0]), reinterpret_cast<float* const*>(dst), st);
+}
+
+// EpsDivDivStokes::apply_impl (epsilon_divdiv_stokes.hpp:55-84): A Replace +
+// Skip into dst.u, B^T Add + communicate into dst.u (one interface sum for both),
+// B Replace + communicate into dst.p. Always Replace, like the reference.
+void StokesOp::apply(void* const* src, void* const* dst, cudaStream_t st)
+{
+    if (apply_mode != 0) throw Error(kErrUnsupported, "the Stokes block operator applies in Replace mode only");
+    void* const su[3] = {src[0], src[1], src[2]};
+    void* const du[3] = {dst[0], dst[1], dst[2]};
+    void* const sp[1] = {src[3]};
+    void* const dp[1] = {dst[3]};
+    A.apply_mode      = 0;
+    A.comm_mode       = 0;
+    A.apply(su, du, st);
+    BT.apply_mode = 1;
+    BT.comm_mode  = comm_mode;
+    BT.apply(sp, du, st);
+    B.apply_mode = apply_mode;
+    B.comm_mode  = comm_mode;
+    B.apply(su, dp, st);
+}
 
 }  // namespace tn

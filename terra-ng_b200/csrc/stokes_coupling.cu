@@ -1,0 +1,357 @@
+// P1-iso-P2 / P1 coupling blocks and mass matrices (FP64 and FP32).
+//
+//   divergence B   : fine velocity (level L) -> coarse pressure (level L-1)
+//                    p_i += -|det J| shape_coarse_i div u   (divergence_kerngen.hpp:519-778)
+//   gradient   B^T : coarse pressure -> fine velocity
+//                    u_{n,d} += -|det J| g_{n,d} p_interp   (gradient_kerngen.hpp:498-759)
+//   lumped k-mass  : diag of the 6-point k-weighted pressure mass (kmass.hpp:98-181)
+//   vector mass    : 6-point mass matrix applied per component (vector_mass.hpp:60-150)
+//
+// One thread per fine cell (threads along r), both wedges, factorised wedge
+// Jacobian as in the epsilon-div-div kernel, contributions added with native
+// FP64/FP32 global atomics. The coarse node of fine wedge node i is
+// (x/2, y/2, r/2) + the fine wedge's node offset, with the reference's
+// shape_coarse(i, r%2, fine_lateral_wedge_idx(x, y, w)) weights; this keeps
+// B and B^T exact transposes of each other and of the reference.
+#include "tn_device.cuh"
+#include "tn_kernels.hpp"
+#include "tn_wedge_math.cuh"
+
+namespace tn {
+namespace {
+
+__host__ __device__ constexpr int woff(int w, int n, int k)
+{
+    // WEDGE_NODE_OFF (kernel_helpers.hpp:291-312)
+    constexpr int t[2][6][3] = {{{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}},
+                                {{1, 1, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 1}, {0, 1, 1}, {1, 0, 1}}};
+    return t[w][n][k];
+}
+
+// fine_lateral_wedge_idx (kernel_helpers.hpp:600-608)
+__host__ __device__ __forceinline__ int fine_lat_wedge(int x, int y, int w)
+{
+    constexpr int idx[2][2][2] = {{{0, 1}, {2, 3}}, {{3, 2}, {1, 0}}};
+    return idx[w][y & 1][x & 1];
+}
+
+// shape_coarse(i, frw, flw, centroid) (integrands.hpp:250-393) at (1/3, 1/3, 0).
+template <typename T>
+__host__ __device__ __forceinline__ T shape_coarse_centroid(int i, int frw, int flw)
+{
+    const T xi = T(1) / T(3), eta = T(1) / T(3);
+    T       lat;
+    switch (i % 3) {
+    case 0:
+        lat = flw == 0 ? T(-0.5) * eta - T(0.5) * xi + T(1) : (flw == 3 ? T(0.5) * eta + T(0.5) * xi : T(-0.5) * eta - T(0.5) * xi + T(0.5));
+        break;
+    case 1: lat = flw == 1 ? T(0.5) * xi + T(0.5) : (flw == 3 ? T(0.5) - T(0.5) * xi : T(0.5) * xi); break;
+    default: lat = flw == 2 ? T(0.5) * eta + T(0.5) : (flw == 3 ? T(0.5) - T(0.5) * eta : T(0.5) * eta); break;
+    }
+    T rad;
+    if (i / 3 == 0)
+        rad = frw == 0 ? T(0.75) : T(0.25);
+    else
+        rad = frw == 0 ? T(0.25) : T(0.75);
+    return lat * rad;
+}
+
+template <typename T>
+struct CouplingArgs {
+    int      nl, nr;  // fine level
+    const T* coords;  // fine unit-sphere coords
+    const T* radii;   // fine radii
+    int      bc_cmb, bc_surf;
+    const T* u[3];    // fine velocity (divergence input / gradient output)
+    T*       uo[3];
+    const T* p;       // coarse pressure (gradient input)
+    T*       po;      // coarse pressure (divergence output)
+};
+
+// Per-cell physical gradients of the six wedge nodes for both wedges.
+template <typename T>
+__device__ __forceinline__ void cell_grads(const T* coords, int nl, int d, int x, int y, T r0, T r1, T (&g)[2][6][3],
+                                           T (&absdet)[2])
+{
+    T geo[20];
+    column_geometry<T>(coords, nl, d, x, y, geo);
+    const T rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+    const T alpha = T(0.5) / rm, beta = T(1) / (T(6) * hdr);
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const T* gw = geo + 10 * w;
+        absdet[w]   = gw[9] * rm * rm * hdr;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int m  = n % 3;
+            const T   sg = n < 3 ? T(-1) : T(1);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
+                g[w][n][i] = alpha * L + sg * beta * gw[6 + i];
+            }
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int x, int y, T (&n)[3])
+{
+    const T* c = coords + lat_index3(nl, d, x, y) * 3;
+    n[0]       = c[0];
+    n[1]       = c[1];
+    n[2]       = c[2];
+}
+
+template <typename T>
+__global__ void divergence_kernel(CouplingArgs<T> A)
+{
+    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    const int r  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y  = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
+    if (r >= nr - 1) return;
+    T g[2][6][3], adet[2];
+    cell_grads<T>(A.coords, nl, d, x, y, A.radii[r], A.radii[r + 1], g, adet);
+    const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
+    const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
+    const int  bside  = at_cmb ? 0 : 1;
+    const int  frw    = r & 1;
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        T div = T(0);
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int  nx = x + woff(w, n, 0), ny = y + woff(w, n, 1), nrr = r + woff(w, n, 2);
+            const bool bn = (at_cmb || at_surf) && (woff(w, n, 2) == bside);
+            if (bcf == 1 && bn) continue;
+            const int64_t id = node_index(nl, nr, d, nx, ny, nrr);
+            T             u0 = A.u[0][id], u1 = A.u[1][id], u2 = A.u[2][id];
+            if (bcf == 2 && bn) {
+                T nn[3];
+                unit_normal<T>(A.coords, nl, d, nx, ny, nn);
+                const T un = u0 * nn[0] + u1 * nn[1] + u2 * nn[2];
+                u0 -= un * nn[0];
+                u1 -= un * nn[1];
+                u2 -= un * nn[2];
+            }
+            div += g[w][n][0] * u0 + g[w][n][1] * u1 + g[w][n][2] * u2;
+        }
+        const T   pre = -adet[w] * div;
+        const int flw = fine_lat_wedge(x, y, w);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const int64_t id =
+                node_index(nlc, nrc, d, x / 2 + woff(w, i, 0), y / 2 + woff(w, i, 1), r / 2 + woff(w, i, 2));
+            atomicAdd(&A.po[id], pre * shape_coarse_centroid<T>(i, frw, flw));
+        }
+    }
+}
+
+template <typename T>
+__global__ void gradient_kernel(CouplingArgs<T> A)
+{
+    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    const int r  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y  = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
+    if (r >= nr - 1) return;
+    T g[2][6][3], adet[2];
+    cell_grads<T>(A.coords, nl, d, x, y, A.radii[r], A.radii[r + 1], g, adet);
+    const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
+    const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
+    const int  bside  = at_cmb ? 0 : 1;
+    const int  frw    = r & 1;
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const int flw = fine_lat_wedge(x, y, w);
+        T         pi  = T(0);
+#pragma unroll
+        for (int j = 0; j < 6; ++j)
+            pi += shape_coarse_centroid<T>(j, frw, flw) *
+                  A.p[node_index(nlc, nrc, d, x / 2 + woff(w, j, 0), y / 2 + woff(w, j, 1), r / 2 + woff(w, j, 2))];
+        const T pre = -adet[w] * pi;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int  nx = x + woff(w, n, 0), ny = y + woff(w, n, 1), nrr = r + woff(w, n, 2);
+            const bool bn = (at_cmb || at_surf) && (woff(w, n, 2) == bside);
+            if (bcf == 1 && bn) continue;
+            T c0 = pre * g[w][n][0], c1 = pre * g[w][n][1], c2 = pre * g[w][n][2];
+            if (bcf == 2 && bn) {
+                T nn[3];
+                unit_normal<T>(A.coords, nl, d, nx, ny, nn);
+                const T cn = c0 * nn[0] + c1 * nn[1] + c2 * nn[2];
+                c0 -= cn * nn[0];
+                c1 -= cn * nn[1];
+                c2 -= cn * nn[2];
+            }
+            const int64_t id = node_index(nl, nr, d, nx, ny, nrr);
+            atomicAdd(&A.uo[0][id], c0);
+            atomicAdd(&A.uo[1][id], c1);
+            atomicAdd(&A.uo[2][id], c2);
+        }
+    }
+}
+
+// Felippa 3x2 rule (quadrature.hpp:57-100).
+__host__ __device__ constexpr double qp6(int q, int k)
+{
+    constexpr double t[6][3] = {{0.6666666666666666, 0.1666666666666667, -0.5773502691896257},
+                                {0.1666666666666667, 0.6666666666666666, -0.5773502691896257},
+                                {0.1666666666666667, 0.1666666666666667, -0.5773502691896257},
+                                {0.6666666666666666, 0.1666666666666667, 0.5773502691896257},
+                                {0.1666666666666667, 0.6666666666666666, 0.5773502691896257},
+                                {0.1666666666666667, 0.1666666666666667, 0.5773502691896257}};
+    return t[q][k];
+}
+
+// 6x6 wedge mass matrix with optional nodal coefficient (kmass.hpp:120-160,
+// vector_mass.hpp:96-130), FP64 accumulation.
+template <typename T>
+__device__ void wedge_mass(const T* coords, int nl, int d, int x, int y, const T* radii, int r, int w, const T* kloc,
+                           double (&M)[6][6])
+{
+    double p[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int q = wedge_corner(w, m);
+        const T*  c = coords + lat_index3(nl, d, x + (q & 1), y + (q >> 1)) * 3;
+        for (int i = 0; i < 3; ++i) p[m][i] = static_cast<double>(c[i]);
+    }
+    const double r1 = radii[r], r2 = radii[r + 1], grad_r = 0.5 * (r2 - r1);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) M[i][j] = 0.0;
+    for (int q = 0; q < 6; ++q) {
+        const double xi = qp6(q, 0), eta = qp6(q, 1), zeta = qp6(q, 2);
+        double       J[3][3];
+        for (int i = 0; i < 3; ++i) {
+            J[i][0] = p[1][i] - p[0][i];
+            J[i][1] = p[2][i] - p[0][i];
+            J[i][2] = (1 - xi - eta) * p[0][i] + xi * p[1][i] + eta * p[2][i];
+        }
+        double dl = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                    J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        dl              = dl < 0 ? -dl : dl;
+        const double rq = r1 + 0.5 * (r2 - r1) * (1 + zeta);
+        double       N[6];
+        const double lat[3] = {1.0 - xi - eta, xi, eta};
+        for (int n = 0; n < 6; ++n) N[n] = lat[n % 3] * (n < 3 ? 0.5 * (1 - zeta) : 0.5 * (1 + zeta));
+        double kev = 1.0;
+        if (kloc) {
+            kev = 0.0;
+            for (int n = 0; n < 6; ++n) kev += N[n] * static_cast<double>(kloc[n]);
+        }
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) M[i][j] += 0.1666666666666667 * kev * (N[i] * N[j] * rq * rq * grad_r * dl);
+    }
+}
+
+template <typename T>
+__global__ void kmass_lumped_kernel(int nl, int nr, const T* coords, const T* radii, const T* k, T* diag)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
+    if (r >= nr - 1) return;
+    for (int w = 0; w < 2; ++w) {
+        T kl[6];
+        for (int n = 0; n < 6; ++n) kl[n] = k[node_index(nl, nr, d, x + woff(w, n, 0), y + woff(w, n, 1), r + woff(w, n, 2))];
+        double M[6][6];
+        wedge_mass<T>(coords, nl, d, x, y, radii, r, w, kl, M);
+        for (int i = 0; i < 6; ++i) {
+            double rs = 0;
+            for (int j = 0; j < 6; ++j) rs += M[i][j];
+            atomicAdd(&diag[node_index(nl, nr, d, x + woff(w, i, 0), y + woff(w, i, 1), r + woff(w, i, 2))],
+                      static_cast<T>(rs));
+        }
+    }
+}
+
+template <typename T>
+__global__ void vector_mass_kernel(int nl, int nr, const T* coords, const T* radii, CouplingArgs<T> A)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
+    if (r >= nr - 1) return;
+    for (int w = 0; w < 2; ++w) {
+        double M[6][6];
+        wedge_mass<T>(coords, nl, d, x, y, radii, r, w, nullptr, M);
+        int64_t id[6];
+        for (int n = 0; n < 6; ++n) id[n] = node_index(nl, nr, d, x + woff(w, n, 0), y + woff(w, n, 1), r + woff(w, n, 2));
+        for (int c = 0; c < 3; ++c)
+            for (int i = 0; i < 6; ++i) {
+                double acc = 0;
+                for (int j = 0; j < 6; ++j) acc += M[i][j] * static_cast<double>(A.u[c][id[j]]);
+                atomicAdd(&A.uo[c][id[i]], static_cast<T>(acc));
+            }
+    }
+}
+
+inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+
+inline dim3 cell_grid(int nl, int nr, int threads) { return dim3((nr - 1 + threads - 1) / threads, (nl - 1) * (nl - 1), 10); }
+
+}  // namespace
+
+template <typename T>
+int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t st)
+{
+    CouplingArgs<T> a{};
+    a.nl = p.nl;
+    a.nr = p.nr;
+    a.coords = p.coords;
+    a.radii  = p.radii;
+    a.bc_cmb = p.bc_cmb;
+    a.bc_surf = p.bc_surf;
+    for (int c = 0; c < 3; ++c) a.u[c] = p.u[c];
+    a.po             = p.p_out;
+    const int thr    = p.nr - 1 >= 64 ? 64 : 32;
+    divergence_kernel<T><<<cell_grid(p.nl, p.nr, thr), thr, 0, st>>>(a);
+    return launch_status();
+}
+
+template <typename T>
+int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t st)
+{
+    CouplingArgs<T> a{};
+    a.nl = p.nl;
+    a.nr = p.nr;
+    a.coords = p.coords;
+    a.radii  = p.radii;
+    a.bc_cmb = p.bc_cmb;
+    a.bc_surf = p.bc_surf;
+    a.p      = p.p_in;
+    for (int c = 0; c < 3; ++c) a.uo[c] = p.u_out[c];
+    const int thr = p.nr - 1 >= 64 ? 64 : 32;
+    gradient_kernel<T><<<cell_grid(p.nl, p.nr, thr), thr, 0, st>>>(a);
+    return launch_status();
+}
+
+template <typename T>
+int kmass_lumped_add(int nl, int nr, const T* coords, const T* radii, const T* k, T* diag, cudaStream_t st)
+{
+    const int thr = nr - 1 >= 64 ? 64 : 32;
+    kmass_lumped_kernel<T><<<cell_grid(nl, nr, thr), thr, 0, st>>>(nl, nr, coords, radii, k, diag);
+    return launch_status();
+}
+
+template <typename T>
+int vector_mass_add(int nl, int nr, const T* coords, const T* radii, const T* const* src, T* const* dst, cudaStream_t st)
+{
+    CouplingArgs<T> a{};
+    for (int c = 0; c < 3; ++c) {
+        a.u[c]  = src[c];
+        a.uo[c] = dst[c];
+    }
+    const int thr = nr - 1 >= 64 ? 64 : 32;
+    vector_mass_kernel<T><<<cell_grid(nl, nr, thr), thr, 0, st>>>(nl, nr, coords, radii, a);
+    return launch_status();
+}
+
+#define TN_INST(T)                                                                                                 \
+    template int divergence_apply<T>(const CouplingLaunch<T>&, cudaStream_t);                                     \
+    template int gradient_apply<T>(const CouplingLaunch<T>&, cudaStream_t);                                       \
+    template int kmass_lumped_add<T>(int, int, const T*, const T*, const T*, T*, cudaStream_t);                  \
+    template int vector_mass_add<T>(int, int, const T*, const T*, const T* const*, T* const*, cudaStream_t);
+TN_INST(double)
+TN_INST(float)
+#undef TN_INST
+
+}  // namespace tn

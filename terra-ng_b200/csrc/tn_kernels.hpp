@@ -30,6 +30,43 @@ template <typename T>
 int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream);
 
 // ----------------------------------------------------------------------------
+// Coupling blocks and mass matrices (stokes_coupling.cu). All accumulate into
+// their outputs (callers zero them for Replace mode).
+// ----------------------------------------------------------------------------
+template <typename T>
+struct CouplingLaunch {
+    int      nl = 0, nr = 0;  // fine (velocity) level
+    const T* coords = nullptr;
+    const T* radii  = nullptr;
+    int      bc_cmb = 1, bc_surf = 1;
+    const T* u[3]     = {nullptr, nullptr, nullptr};  // divergence input
+    T*       p_out    = nullptr;                      // divergence output (coarse)
+    const T* p_in     = nullptr;                      // gradient input (coarse)
+    T*       u_out[3] = {nullptr, nullptr, nullptr};  // gradient output
+};
+template <typename T>
+int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t stream);
+template <typename T>
+int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t stream);
+template <typename T>
+int kmass_lumped_add(int nl, int nr, const T* coords, const T* radii, const T* k, T* diag, cudaStream_t stream);
+template <typename T>
+int vector_mass_add(int nl, int nr, const T* coords, const T* radii, const T* const* src, T* const* dst,
+                    cudaStream_t stream);
+
+// ----------------------------------------------------------------------------
+// Constant-weight grid transfers (transfer.cu). Levels given by the fine grid.
+// prolongate_add: fine += P coarse (gather per fine node).
+// restrict_owned: coarse = sum over owned fine neighbours (weights of
+//                 prolongation_constant_weight); the interface sum follows.
+// ----------------------------------------------------------------------------
+template <typename T>
+int prolongate_add(int nlf, int nrf, int ncomp, const T* const* coarse, T* const* fine, cudaStream_t stream);
+template <typename T>
+int restrict_owned(int nlf, int nrf, int ncomp, const uint8_t* owned_lat_fine, const T* const* fine, T* const* coarse,
+                   cudaStream_t stream);
+
+// ----------------------------------------------------------------------------
 // Interface sum over diamond-edge duplicates (vector_ops.cu).
 // classes: offsets (num_classes + 1) into members (lateral indices).
 // ----------------------------------------------------------------------------

@@ -156,23 +156,69 @@ struct Shell {
 
 std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, double r_min, double r_max);
 
-// epsilon-div-div operator object (EpsilonDivDivKerngen).
-struct EpsDivDivOp {
+// Operator objects behind tn_operator. Vector arguments are arrays of
+// component pointers: velocity = 3 components, pressure = 1, Stokes = 4
+// (u_x, u_y, u_z, p). Every apply honours the apply mode (Replace / Add) and the
+// communication mode (interface sum of the output or not).
+struct Operator {
     const Shell* shell = nullptr;
-    int          level = 0;
+    int          level = 0;      // velocity (fine) level index
     int          precision = 0;  // 0 f64, 1 f32
-    DevBuf       k;               // nodal or cell coefficient in `precision`
-    bool         q0 = false;
+    int          apply_mode = 0; // 0 replace, 1 add
+    int          comm_mode  = 1; // 1 communicate additively
     int          bc_cmb = 1, bc_surf = 1;
-    bool         diagonal = false;
-    int          apply_mode = 0;  // 0 replace, 1 add
-    int          comm_mode  = 1;  // 1 communicate additively
-    int          tile_y = 0, chunk_x = 0;
 
+    virtual ~Operator() = default;
+    virtual int  src_components() const = 0;
+    virtual int  dst_components() const = 0;
+    virtual bool dst_on_coarse() const { return false; }
+    virtual void apply(void* const* src, void* const* dst, cudaStream_t st) = 0;
     const DeviceLevel& lvl() const { return shell->level(level); }
-    // dst = A src (mode Replace) / dst += A src (mode Add); interface sum if comm.
-    template <typename T>
-    void apply(const T* const* src, T* const* dst, cudaStream_t st, bool diag_override = false) const;
 };
+
+// epsilon-div-div (EpsilonDivDivKerngen).
+struct EpsDivDivOp : Operator {
+    DevBuf k;  // nodal or cell coefficient in `precision`
+    bool   q0 = false;
+    bool   diagonal = false;
+    int    tile_y = 0, chunk_x = 0;
+    int    src_components() const override { return 3; }
+    int    dst_components() const override { return 3; }
+    void   apply(void* const* src, void* const* dst, cudaStream_t st) override;
+    template <typename T>
+    void apply_t(const T* const* src, T* const* dst, cudaStream_t st) const;
+};
+
+// B (DivergenceKerngen): velocity level -> pressure level (level - 1).
+struct DivergenceOp : Operator {
+    int  src_components() const override { return 3; }
+    int  dst_components() const override { return 1; }
+    bool dst_on_coarse() const override { return true; }
+    void apply(void* const* src, void* const* dst, cudaStream_t st) override;
+    template <typename T>
+    void apply_t(const T* const* src, T* p, cudaStream_t st) const;
+};
+
+// B^T (GradientKerngen): pressure level -> velocity level.
+struct GradientOp : Operator {
+    int  src_components() const override { return 1; }
+    int  dst_components() const override { return 3; }
+    void apply(void* const* src, void* const* dst, cudaStream_t st) override;
+    template <typename T>
+    void apply_t(const T* p, T* const* dst, cudaStream_t st) const;
+};
+
+// [A B^T; B 0] (EpsDivDivStokes, epsilon_divdiv_stokes.hpp:55-84).
+struct StokesOp : Operator {
+    EpsDivDivOp  A;
+    GradientOp   BT;
+    DivergenceOp B;
+    int          src_components() const override { return 4; }
+    int          dst_components() const override { return 4; }
+    void         apply(void* const* src, void* const* dst, cudaStream_t st) override;
+};
+
+template <typename T>
+void zero_components(int64_t n, int ncomp, T* const* v, cudaStream_t st);
 
 }  // namespace tn

@@ -1,0 +1,144 @@
+// Constant-weight multigrid transfers between level l (fine) and l-1 (coarse).
+//
+// Weights are prolongation_constant_weight (fe/wedge/shell/
+// grid_transfer_constant.hpp:24-89): linear interpolation on the anti-diagonal
+// triangulation of each diamond, tensor product with linear interpolation in r.
+//   prolongate_add : fine += P coarse   (ProlongationVecConstant, Add mode,
+//                    prolongation_constant.hpp:146-191), here as a gather: one
+//                    thread per fine node reading its 1..8 coarse parents, no atomics.
+//   restrict_owned : coarse = P^T (owned fine)  (RestrictionVecConstant,
+//                    restriction_constant.hpp:190-249): one thread per coarse
+//                    node over its 21-point fine stencil, non-owned fine
+//                    duplicates masked; the caller completes it with the coarse
+//                    interface sum.
+#include "tn_device.cuh"
+#include "tn_kernels.hpp"
+#include "tn_wedge_math.cuh"
+
+namespace tn {
+namespace {
+
+constexpr int kMaxComp = 4;
+template <typename T>
+struct PtrSet {
+    const T* in[kMaxComp];
+    T*       out[kMaxComp];
+};
+
+template <typename T>
+__global__ void prolongate_kernel(int nlf, int nrf, int ncomp, PtrSet<T> P)
+{
+    const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
+    const int r   = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y   = blockIdx.y % nlf, x = blockIdx.y / nlf, d = blockIdx.z;
+    if (r >= nrf) return;
+    // lateral parents (at most two) with weights
+    int xa[2], ya[2], nlat;
+    if ((x & 1) == 0 && (y & 1) == 0) {
+        xa[0] = x / 2;
+        ya[0] = y / 2;
+        nlat  = 1;
+    } else if ((y & 1) == 0) {
+        xa[0] = (x - 1) / 2, ya[0] = y / 2;
+        xa[1] = (x + 1) / 2, ya[1] = y / 2;
+        nlat  = 2;
+    } else if ((x & 1) == 0) {
+        xa[0] = x / 2, ya[0] = (y - 1) / 2;
+        xa[1] = x / 2, ya[1] = (y + 1) / 2;
+        nlat  = 2;
+    } else {
+        xa[0] = (x + 1) / 2, ya[0] = (y - 1) / 2;
+        xa[1] = (x - 1) / 2, ya[1] = (y + 1) / 2;
+        nlat  = 2;
+    }
+    int       ra[2], nrad;
+    const T   wl = nlat == 1 ? T(1) : T(0.5);
+    if ((r & 1) == 0) {
+        ra[0] = r / 2;
+        nrad  = 1;
+    } else {
+        ra[0] = (r - 1) / 2;
+        ra[1] = (r + 1) / 2;
+        nrad  = 2;
+    }
+    const T       wr = nrad == 1 ? T(1) : T(0.5);
+    const int64_t fi = node_index(nlf, nrf, d, x, y, r);
+    for (int c = 0; c < ncomp; ++c) {
+        T acc = T(0);
+        for (int a = 0; a < nlat; ++a)
+            for (int b = 0; b < nrad; ++b) acc += P.in[c][node_index(nlc, nrc, d, xa[a], ya[a], ra[b])];
+        P.out[c][fi] += wl * wr * acc;
+    }
+}
+
+template <typename T>
+__global__ void restrict_kernel(int nlf, int nrf, int ncomp, const uint8_t* __restrict__ owned, PtrSet<T> P)
+{
+    const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
+    const int rc  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int yc  = blockIdx.y % nlc, xc = blockIdx.y / nlc, d = blockIdx.z;
+    if (rc >= nrc) return;
+    // 7-point lateral stencil (prolongation_constant_fine_grid_stencil_offsets_at_coarse_vertex)
+    constexpr int ox[7] = {-1, -1, 0, 1, 1, 0, 0};
+    constexpr int oy[7] = {0, 1, 1, 0, -1, -1, 0};
+    T             acc[kMaxComp];
+    for (int c = 0; c < ncomp; ++c) acc[c] = T(0);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) {
+        const int xf = 2 * xc + ox[o], yf = 2 * yc + oy[o];
+        if (xf < 0 || xf >= nlf || yf < 0 || yf >= nlf) continue;
+        if (!owned[lat_index3(nlf, d, xf, yf)]) continue;
+        const T wl = (o == 6) ? T(1) : T(0.5);
+#pragma unroll
+        for (int dr = -1; dr <= 1; ++dr) {
+            const int rf = 2 * rc + dr;
+            if (rf < 0 || rf >= nrf) continue;
+            const T       wgt = dr == 0 ? wl : T(0.5) * wl;
+            const int64_t fi  = node_index(nlf, nrf, d, xf, yf, rf);
+            for (int c = 0; c < ncomp; ++c) acc[c] += wgt * P.in[c][fi];
+        }
+    }
+    const int64_t ci = node_index(nlc, nrc, d, xc, yc, rc);
+    for (int c = 0; c < ncomp; ++c) P.out[c][ci] = acc[c];
+}
+
+inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+
+}  // namespace
+
+template <typename T>
+int prolongate_add(int nlf, int nrf, int ncomp, const T* const* coarse, T* const* fine, cudaStream_t st)
+{
+    if (ncomp < 1 || ncomp > kMaxComp) return -1;
+    PtrSet<T> P{};
+    for (int c = 0; c < ncomp; ++c) {
+        P.in[c]  = coarse[c];
+        P.out[c] = fine[c];
+    }
+    const int thr = nrf >= 64 ? 64 : 32;
+    prolongate_kernel<T><<<dim3((nrf + thr - 1) / thr, nlf * nlf, 10), thr, 0, st>>>(nlf, nrf, ncomp, P);
+    return launch_status();
+}
+
+template <typename T>
+int restrict_owned(int nlf, int nrf, int ncomp, const uint8_t* owned_lat_fine, const T* const* fine, T* const* coarse,
+                   cudaStream_t st)
+{
+    if (ncomp < 1 || ncomp > kMaxComp) return -1;
+    PtrSet<T> P{};
+    for (int c = 0; c < ncomp; ++c) {
+        P.in[c]  = fine[c];
+        P.out[c] = coarse[c];
+    }
+    const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
+    const int thr = nrc >= 64 ? 64 : 32;
+    restrict_kernel<T><<<dim3((nrc + thr - 1) / thr, nlc * nlc, 10), thr, 0, st>>>(nlf, nrf, ncomp, owned_lat_fine, P);
+    return launch_status();
+}
+
+template int prolongate_add<double>(int, int, int, const double* const*, double* const*, cudaStream_t);
+template int prolongate_add<float>(int, int, int, const float* const*, float* const*, cudaStream_t);
+template int restrict_owned<double>(int, int, int, const uint8_t*, const double* const*, double* const*, cudaStream_t);
+template int restrict_owned<float>(int, int, int, const uint8_t*, const float* const*, float* const*, cudaStream_t);
+
+}  // namespace tn

@@ -64,6 +64,14 @@ def load(path: str = LIB_PATH):
         "tn_operator_set_boundary_conditions": ([vp, i, i], i),
         "tn_operator_set_tile": ([vp, i, i], i),
         "tn_operator_apply": ([vp, vpp, vpp, vp], i),
+        "tn_divergence_create": ([vp, i, i, i, i, ctypes.POINTER(vp)], i),
+        "tn_gradient_create": ([vp, i, i, i, i, ctypes.POINTER(vp)], i),
+        "tn_stokes_create": ([vp, i, i, vp, vp, i, i, ctypes.POINTER(vp)], i),
+        "tn_operator_components": ([vp, ctypes.POINTER(i), ctypes.POINTER(i)], i),
+        "tn_kmass_lumped_diagonal": ([vp, i, i, vp, vp, vp], i),
+        "tn_vector_mass_apply": ([vp, i, i, vpp, vpp, vp], i),
+        "tn_prolongate_add": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_restrict": ([vp, i, i, i, vpp, vpp, vp], i),
         "tn_interface_sum": ([vp, i, i, i, vpp, vp], i),
         "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
         "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
@@ -232,8 +240,38 @@ def mesh_generate_host(lat_level: int, rad_level: int, r_min=0.55, r_max=1.0):
     return coords, radii, owned, cls, n.value
 
 
-class EpsDivDiv:
-    """epsilon-div-div operator (tn_epsdivdiv_* / tn_operator_*)."""
+class Operator:
+    """Common part of the operator handles (tn_operator_*)."""
+
+    _h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tn_operator_destroy(self._h)
+            self._h = None
+
+    def _adopt(self, h):
+        self._h = h
+        si, di = ctypes.c_int(), ctypes.c_int()
+        _check(load().tn_operator_components(h, ctypes.byref(si), ctypes.byref(di)))
+        self.src_components, self.dst_components = si.value, di.value
+
+    def set_modes(self, apply_mode=REPLACE, comm_mode=COMMUNICATE_ADDITIVELY):
+        _check(load().tn_operator_set_modes(self._h, apply_mode, comm_mode))
+
+    def set_boundary_conditions(self, bc_cmb, bc_surface):
+        _check(load().tn_operator_set_boundary_conditions(self._h, bc_cmb, bc_surface))
+
+    def apply(self, src, dst, stream=None):
+        cs, cd = _comps(src), _comps(dst)
+        if len(cs) != self.src_components or len(cd) != self.dst_components:
+            raise ValueError(f"operator takes {self.src_components} -> {self.dst_components} components")
+        _check(load().tn_operator_apply(self._h, _ptrs(cs), _ptrs(cd), _stream(stream)))
+        return dst
+
+
+class EpsDivDiv(Operator):
+    """epsilon-div-div operator (tn_epsdivdiv_create)."""
 
     def __init__(self, shell: Shell, level: int = -1, k=None, k_cell=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET,
                  diagonal=False):
@@ -248,28 +286,80 @@ class EpsDivDiv:
         kc = ctypes.c_void_p(k_cell.data_ptr()) if k_cell is not None else None
         _check(L.tn_epsdivdiv_create(shell.handle, self.level, _prec(self.dtype), kp, kc, bc_cmb, bc_surface,
                                      int(diagonal), ctypes.byref(h)))
-        self._h = h
-
-    def __del__(self):
-        if getattr(self, "_h", None) and _lib is not None:
-            _lib.tn_operator_destroy(self._h)
-            self._h = None
-
-    def set_modes(self, apply_mode=REPLACE, comm_mode=COMMUNICATE_ADDITIVELY):
-        _check(load().tn_operator_set_modes(self._h, apply_mode, comm_mode))
+        self._adopt(h)
 
     def set_diagonal(self, flag: bool):
         _check(load().tn_operator_set_diagonal(self._h, int(flag)))
 
-    def set_boundary_conditions(self, bc_cmb, bc_surface):
-        _check(load().tn_operator_set_boundary_conditions(self._h, bc_cmb, bc_surface))
-
     def set_tile(self, tile_y=0, chunk_x=0):
         _check(load().tn_operator_set_tile(self._h, tile_y, chunk_x))
 
-    def apply(self, src, dst, stream=None):
-        cs, cd = _comps(src), _comps(dst)
-        if len(cs) != 3 or len(cd) != 3:
-            raise ValueError("velocity vectors need three components")
-        _check(load().tn_operator_apply(self._h, _ptrs(cs), _ptrs(cd), _stream(stream)))
-        return dst
+
+class Divergence(Operator):
+    """B: velocity on `level` -> pressure on `level - 1` (tn_divergence_create)."""
+
+    def __init__(self, shell: Shell, level: int = -1, dtype=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET):
+        import torch
+
+        self.shell, self.level = shell, level % shell.num_levels
+        h = ctypes.c_void_p()
+        _check(load().tn_divergence_create(shell.handle, self.level, _prec(dtype or torch.float64), bc_cmb,
+                                           bc_surface, ctypes.byref(h)))
+        self._adopt(h)
+
+
+class Gradient(Operator):
+    """B^T: pressure on `level - 1` -> velocity on `level` (tn_gradient_create)."""
+
+    def __init__(self, shell: Shell, level: int = -1, dtype=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET):
+        import torch
+
+        self.shell, self.level = shell, level % shell.num_levels
+        h = ctypes.c_void_p()
+        _check(load().tn_gradient_create(shell.handle, self.level, _prec(dtype or torch.float64), bc_cmb, bc_surface,
+                                         ctypes.byref(h)))
+        self._adopt(h)
+
+
+class Stokes(Operator):
+    """[A B^T; B 0] on (velocity level, level - 1) (tn_stokes_create); vectors are 4 components."""
+
+    def __init__(self, shell: Shell, level: int = -1, k=None, k_cell=None, bc_cmb=DIRICHLET, bc_surface=DIRICHLET):
+        if (k is None) == (k_cell is None):
+            raise ValueError("give exactly one of k (nodal) or k_cell (Q0)")
+        ref = k if k is not None else k_cell
+        self.shell, self.level = shell, level % shell.num_levels
+        h = ctypes.c_void_p()
+        kp = ctypes.c_void_p(k.data_ptr()) if k is not None else None
+        kc = ctypes.c_void_p(k_cell.data_ptr()) if k_cell is not None else None
+        _check(load().tn_stokes_create(shell.handle, self.level, _prec(ref.dtype), kp, kc, bc_cmb, bc_surface,
+                                       ctypes.byref(h)))
+        self._adopt(h)
+
+
+def kmass_lumped_diagonal(shell: Shell, level: int, k, out, stream=None):
+    _check(load().tn_kmass_lumped_diagonal(shell.handle, level % shell.num_levels, _prec(k.dtype),
+                                           ctypes.c_void_p(k.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                           _stream(stream)))
+    return out
+
+
+def vector_mass_apply(shell: Shell, level: int, src, dst, stream=None):
+    cs, cd = _comps(src), _comps(dst)
+    _check(load().tn_vector_mass_apply(shell.handle, level % shell.num_levels, _prec(cs[0].dtype), _ptrs(cs),
+                                       _ptrs(cd), _stream(stream)))
+    return dst
+
+
+def prolongate_add(shell: Shell, fine_level: int, coarse, fine, stream=None):
+    cc, cf = _comps(coarse), _comps(fine)
+    _check(load().tn_prolongate_add(shell.handle, fine_level % shell.num_levels, _prec(cc[0].dtype), len(cc),
+                                    _ptrs(cc), _ptrs(cf), _stream(stream)))
+    return fine
+
+
+def restrict(shell: Shell, fine_level: int, fine, coarse, stream=None):
+    cf, cc = _comps(fine), _comps(coarse)
+    _check(load().tn_restrict(shell.handle, fine_level % shell.num_levels, _prec(cf[0].dtype), len(cf), _ptrs(cf),
+                              _ptrs(cc), _stream(stream)))
+    return coarse

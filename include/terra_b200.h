@@ -48,8 +48,12 @@ enum { TN_NEUMANN = 0, TN_DIRICHLET = 1, TN_FREESLIP = 2 };
 enum { TN_REPLACE = 0, TN_ADD = 1 };
 enum { TN_SKIP_COMMUNICATION = 0, TN_COMMUNICATE_ADDITIVELY = 1 };
 
+/* OperatorStoredMatrixMode (src/terra/linalg/operator.hpp:29-51); Selective is not provided */
+enum { TN_STORED_OFF = 0, TN_STORED_FULL = 1 };
+
 typedef struct tn_shell    tn_shell;
 typedef struct tn_operator tn_operator;
+typedef struct tn_solver   tn_solver;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* tn_last_error(void);
@@ -158,6 +162,100 @@ int tn_vec_lincomb(tn_shell* shell, int level, int precision, int ncomp, void* c
  * grid_operations.hpp:630-673). Synchronous on `stream`. */
 int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev,
                const void* const* b_dev, double* result, void* stream);
+
+/* Uniform(-1, 1) values from SplitMix64 of (seed, canonical node, component):
+ * the canonical node is the lowest lateral index of the node's duplicate class
+ * times nr plus r, so interface duplicates receive equal values. Stands in for
+ * randomize (grid_operations.hpp:748-773), whose stream depends on the backend. */
+int tn_vec_random(tn_shell* shell, int level, int precision, int ncomp, uint64_t seed, void* const* comps_dev,
+                  void* stream);
+
+/* ---- stored element matrices and Galerkin coarse operators -----------------
+ * set_stored_matrix_mode (epsilon_divdiv_kerngen.hpp:483-528) with
+ * TN_STORED_FULL: assemble and keep the element matrices of the operator's
+ * level from its FP64 coefficient (assemble_local_matrix, :2315-2392); the
+ * apply then runs over the stored matrices with the boundary treatment of the
+ * slow path (:1013-1242). TN_STORED_OFF returns to the matrix-free kernel.
+ * Synchronous. */
+int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream);
+/* TwoGridGCA (src/terra/linalg/solvers/gca/gca.hpp:41-531): coarse (an
+ * epsilon-div-div operator on level l-1 of the same shell) receives stored
+ * matrices sum P^T A_f P over the 16 fine wedges of each coarse hex, A_f the
+ * fine operator's stored matrices or its on-the-fly Neumann element matrices
+ * (FP64 coefficient). The coarse operator applies in its own precision.
+ * Synchronous. */
+int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream);
+/* get_local_matrix for every cell: host array (10, nl-1, nl-1, nr-1, 2, 18, 18),
+ * dimension-wise ordering (row = node + 6 * component), without boundary
+ * treatment. Synchronous. */
+int tn_operator_copy_local_matrices(tn_operator* op, double* mats_host);
+
+/* ---- solvers ----------------------------------------------------------------
+ * Options of the Stokes FGMRES / velocity CG and of the multigrid
+ * preconditioner (FGMRESOptions, fgmres.hpp:13-28; IterativeSolverParameters;
+ * StokesSolverParameters, apps/mantlecirculation/src/parameters.hpp:154-184). */
+typedef struct tn_solver_options {
+    int      restart;                   /* FGMRES(m), 1..64 (30) */
+    int      max_iterations;            /* outer iterations (300) */
+    double   relative_tolerance;        /* 1e-8 */
+    double   absolute_tolerance;        /* 1e-12 */
+    int      chebyshev_order;           /* 2 */
+    int      chebyshev_iterations;      /* pre- and post-smoothing steps (2) */
+    int      power_iterations;          /* lambda_max estimate of D^-1 A (10) */
+    int      num_vcycles;               /* V-cycles per preconditioner call (1) */
+    int      coarse_max_iterations;     /* coarsest-level CG (50) */
+    double   coarse_relative_tolerance; /* 1e-6 */
+    double   coarse_absolute_tolerance; /* 1e-16 */
+    int      gca;                       /* 1: Galerkin coarse operators on all coarse levels, 0: rediscretised (1) */
+    int      mixed_precision;           /* 1: FP32 V-cycle inside the FP64 outer iteration (0) */
+    uint64_t seed;                      /* power-iteration start vectors (12345) */
+    int      normalize_pressure;        /* Stokes: subtract the owned-node pressure mean after the solve, as
+                                           StokesContext::solve does (stokes_solver.hpp:684-690) (1) */
+} tn_solver_options;
+void tn_solver_options_default(tn_solver_options* opts);
+/* Stokes solve on velocity_level / velocity_level-1 (StokesContext,
+ * apps/mantlecirculation/src/stokes_solver.hpp:325-609): FGMRES(m) with the
+ * block-triangular preconditioner (block_preconditioner_2x2.hpp:205-221),
+ * Schur block = inverse lumped KMass with k = 1/eta, velocity block = GMG
+ * V-cycle (Chebyshev-Jacobi smoother, constant transfers, coarsest CG on
+ * level 0). Exactly one of eta_nodal_dev (10,nl,nl,nr) and eta_cell_dev
+ * (10,nl-1,nl-1,nr-1) is given (FP64, copied). k_schur_dev: nodal k on the
+ * pressure level or NULL (then 1/eta at the pressure nodes; required with
+ * eta_cell_dev). Levels 0..velocity_level of the shell form the hierarchy.
+ * Synchronous setup (GCA build, diagonals, power iterations). */
+int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,
+                            const double* eta_cell_dev, const double* k_schur_dev, int bc_cmb, int bc_surface,
+                            const tn_solver_options* opts, void* stream, tn_solver** out);
+/* Velocity-only CG (pcg.hpp:81-169) preconditioned by the same multigrid. */
+int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+                              int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
+                              tn_solver** out);
+void tn_solver_destroy(tn_solver* solver);
+/* solve_impl(A, x, b): x_dev holds the initial guess and receives the
+ * solution; 4 components (u_x, u_y, u_z, p) for a Stokes solver, 3 for a
+ * velocity solver. Synchronous. TN_ERR_NOT_CONVERGED when the iteration limit
+ * or a breakdown stopped it first (x_dev then holds the last iterate). */
+int tn_solver_solve(tn_solver* solver, double* const* x_dev, const double* const* b_dev, void* stream);
+/* Iterations (preconditioner applications), final relative residual
+ * ||b - A x|| / ||b - A x0|| and whether the tolerance was met. */
+int tn_solver_result(const tn_solver* solver, int* iterations, double* relative_residual, int* converged);
+/* Relative residual per iteration (history[0] = 1); *length = entries available. */
+int tn_solver_history(const tn_solver* solver, double* history_host, int capacity, int* length);
+/* z = M^-1 v: the block preconditioner (Stokes, 4 components) or the
+ * multigrid from z = 0 (velocity, 3 components). Synchronous. */
+int tn_solver_precondition(tn_solver* solver, const double* const* v_dev, double* const* z_dev, void* stream);
+/* num_vcycles V-cycles on A x = b of the velocity hierarchy in TN_F64 or TN_F32
+ * (TN_F32 needs mixed_precision); x in/out. Synchronous. */
+int tn_solver_vcycle(tn_solver* solver, int precision, void* const* x_dev, const void* const* b_dev, void* stream);
+/* lambda_max(D^-1 A) of the Chebyshev smoother on level 1..fine. */
+int tn_solver_level_lambda(tn_solver* solver, int level, double* lambda_max);
+/* inverse diagonal used by the smoother on level 1..fine (3 components). */
+int tn_solver_inverse_diagonal(tn_solver* solver, int level, double* const* out_dev, void* stream);
+/* [iterations, initial residual, final residual] of the last coarsest CG. */
+int tn_solver_coarse_stats(tn_solver* solver, double* stats3);
+/* stored matrices of coarse level 0..fine-1 of the hierarchy, layout as
+ * tn_operator_copy_local_matrices. */
+int tn_solver_level_matrices(tn_solver* solver, int level, double* mats_host);
 
 #ifdef __cplusplus
 }

@@ -386,13 +386,17 @@ class Chebyshev:
 
 
 def pcg(A, x, b, dot, max_iter, rtol, atol=1e-16, precond=None, history=None):
-    """pcg.hpp:81-169."""
+    """pcg.hpp:81-169. ``precond(z, r)`` returns the new z; like the
+    reference's solve(preconditioner_, A, z_, r_) it receives the previous z
+    (zeros at the start), which only matters for preconditioners that use it
+    as an initial guess (multigrid)."""
     r = b - A(x)
-    z = r.copy() if precond is None else precond(r)
+    z = np.zeros_like(r)
+    z = r.copy() if precond is None else precond(z, r)
     p = z.copy()
     init = math.sqrt(dot(r, r))
     if history is not None:
-        history.append(init)
+        history.append(1.0)
     if init < atol:
         return x
     for it in range(1, max_iter + 1):
@@ -406,10 +410,10 @@ def pcg(A, x, b, dot, max_iter, rtol, atol=1e-16, precond=None, history=None):
         r = r - alpha * ap
         res = math.sqrt(dot(r, r))
         if history is not None:
-            history.append(res)
+            history.append(res / init)
         if res / init <= rtol or res < atol:
             return x
-        z = r.copy() if precond is None else precond(r)
+        z = r.copy() if precond is None else precond(z, r)
         bn = dot(z, r)
         if abs(an) < np.finfo(np.float64).tiny:
             return x
@@ -531,3 +535,121 @@ def fgmres(A, x, b, dot, precond, restart, rtol, atol, max_iter, history=None):
 # --------------------------------------------------------------------------
 def seeded_normal(shape, seed):
     return np.random.default_rng(seed).standard_normal(shape)
+
+
+def seeded_uniform(shell: Shell, ncomp: int, seed: int):
+    """Uniform(-1, 1) per (seed, canonical node, component) from SplitMix64,
+    the canonical node being the lowest lateral index of the node's duplicate
+    class times nr plus r (duplicates get equal values)."""
+    nl, nr = shell.nl, shell.nr
+    nlat = 10 * nl * nl
+    canon = np.arange(nlat, dtype=np.int64)
+    cls = shell.classes.reshape(-1)
+    for k in range(shell.num_classes):
+        m = np.where(cls == k)[0]
+        canon[m] = m.min()
+    u64 = np.uint64
+    gid_node = canon[:, None].astype(u64) * u64(nr) + np.arange(nr, dtype=u64)[None, :]
+    out = np.empty((ncomp, nlat, nr))
+    with np.errstate(over="ignore"):
+        for c in range(ncomp):
+            gid = gid_node * u64(ncomp) + u64(c)
+            z = u64(seed) + (gid + u64(1)) * u64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> u64(30))) * u64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> u64(27))) * u64(0x94D049BB133111EB)
+            z = z ^ (z >> u64(31))
+            out[c] = 2.0 * ((z >> u64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)) - 1.0
+    return out.reshape(ncomp, 10, nl, nl, nr)
+
+
+def inject(coarse: Shell, fine_field):
+    """coarse(d, x, y, r) = fine(d, 2x, 2y, 2r)."""
+    return np.ascontiguousarray(fine_field[:, ::2, ::2, ::2])
+
+
+class VelocityHierarchy:
+    """Multigrid hierarchy as the product builds it (levels[0] coarsest):
+    GCA coarse operators (TwoGridGCA top-down, stokes_solver.hpp:375-389) or
+    rediscretised ones (injected nodal coefficient), inverse diagonals from
+    the diagonal mode, and Chebyshev smoothers with given lambda_max values."""
+
+    def __init__(self, fine: Shell, k, bc_cmb, bc_surface, num_levels, gca=True, lambdas=None, cheb_order=2,
+                 cheb_iters=2, coarse_max_iter=50, coarse_rtol=1e-6, coarse_atol=1e-16):
+        shells = [fine]
+        for _ in range(num_levels - 1):
+            shells.insert(0, shells[0].coarser())
+        self.shells = shells
+        ops = [None] * num_levels
+        ops[-1] = EpsDivDiv(fine, k=k, bc_cmb=bc_cmb, bc_surface=bc_surface)
+        self.mats = [None] * num_levels
+        kk = k
+        for l in range(num_levels - 2, -1, -1):
+            if gca:
+                if l == num_levels - 2:
+                    src = EpsDivDiv(shells[l + 1], k=k, bc_cmb=NEUMANN, bc_surface=NEUMANN)
+                    m = gca_coarsen(src)
+                else:
+                    src = EpsDivDiv(shells[l + 1], k=np.ones(shells[l + 1].scalar_shape), stored=self.mats[l + 1])
+                    m = gca_coarsen(src, fine_mats=self.mats[l + 1])
+                self.mats[l] = m
+                ops[l] = EpsDivDiv(shells[l], k=np.ones(shells[l].scalar_shape), bc_cmb=bc_cmb, bc_surface=bc_surface,
+                                   stored=m)
+            else:
+                kk = inject(shells[l], kk)
+                ops[l] = EpsDivDiv(shells[l], k=kk, bc_cmb=bc_cmb, bc_surface=bc_surface)
+        self.ops = ops
+        self.inv_diag = [None] + [1.0 / ops[l].diag() for l in range(1, num_levels)]
+        self.lambdas = lambdas
+        self.cheb_order, self.cheb_iters = cheb_order, cheb_iters
+        self.coarse = (coarse_max_iter, coarse_rtol, coarse_atol)
+
+    def apply(self, l, u):
+        return self.ops[l].apply(u, path="slow" if self.ops[l].stored is None else "fast")
+
+    def power_iteration(self, l, start, iterations):
+        return power_iteration(lambda v: self.apply(l, v) * self.inv_diag[l], start, self.shells[l].dot, iterations)
+
+    def multigrid(self, num_cycles=1):
+        n = len(self.shells)
+        smoothers = [None] + [Chebyshev(self.cheb_order, self.inv_diag[l], self.cheb_iters, self.lambdas[l])
+                              for l in range(1, n)]
+        ops = [(lambda v, l=l: self.apply(l, v)) for l in range(n)]
+        it, rtol, atol = self.coarse
+        coarse = lambda A, x, b: pcg(A, x, b, self.shells[0].dot, it, rtol, atol)
+        return Multigrid(ops, self.shells, smoothers, coarse, num_cycles)
+
+
+class StokesSystem:
+    """[A B^T; B 0] on flat block vectors (u raveled, then p) with the
+    block-triangular preconditioner (block_preconditioner_2x2.hpp:205-221)."""
+
+    def __init__(self, fine: Shell, k, bc_cmb, bc_surface, hierarchy: VelocityHierarchy, k_schur=None):
+        self.sh, self.shp = fine, fine.coarser()
+        self.A = EpsDivDiv(fine, k=k, bc_cmb=bc_cmb, bc_surface=bc_surface)
+        self.B = Divergence(fine, bc_cmb=bc_cmb, bc_surface=bc_surface)
+        self.nu = int(np.prod(fine.vec_shape))
+        kp = k_schur if k_schur is not None else 1.0 / inject(self.shp, k)
+        self.inv_schur = 1.0 / kmass_lumped(self.shp, kp)
+        self.mg = hierarchy.multigrid()
+
+    def split(self, v):
+        return v[: self.nu].reshape(self.sh.vec_shape), v[self.nu:].reshape(self.shp.scalar_shape)
+
+    def join(self, u, p):
+        return np.concatenate([np.ravel(u), np.ravel(p)])
+
+    def apply(self, v):
+        u, p = self.split(v)
+        return self.join(self.A.apply(u) + self.B.apply_transpose(p), self.B.apply(u))
+
+    def dot(self, a, b):
+        ua, pa = self.split(a)
+        ub, pb = self.split(b)
+        return self.sh.dot(ua, ub) + self.shp.dot(pa, pb)
+
+    def precondition(self, v):
+        vu, vp = self.split(v)
+        zp = self.inv_schur * vp
+        t = self.B.apply_transpose(zp) + vu
+        zu = self.mg.solve(np.zeros_like(vu), t)
+        return self.join(zu, -zp)

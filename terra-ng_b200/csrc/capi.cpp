@@ -4,13 +4,19 @@
 #include <string>
 
 #include "../../include/terra_b200.h"
-#include "tn_runtime.hpp"
+#include "tn_solver.hpp"
 
 struct tn_shell {
     std::unique_ptr<tn::Shell> impl;
 };
 struct tn_operator {
     std::unique_ptr<tn::Operator> op;
+};
+struct tn_solver {
+    tn_shell*                           shell = nullptr;
+    std::unique_ptr<tn::StokesSolver>   stokes;
+    std::unique_ptr<tn::VelocitySolver> velocity;
+    tn::VelocityMultigrid&              mg() { return stokes ? stokes->mg() : velocity->mg(); }
 };
 
 namespace {
@@ -89,6 +95,43 @@ void init_coupling(Op& o, tn::Shell* sh, int level, int precision, int bc_cmb, i
     o.precision = precision;
     o.bc_cmb    = bc_cmb;
     o.bc_surf   = bc_surface;
+}
+
+tn::MgOptions mg_options(const tn_solver_options& o)
+{
+    tn::MgOptions m;
+    m.cheb_order      = o.chebyshev_order;
+    m.cheb_iters      = o.chebyshev_iterations;
+    m.power_iters     = o.power_iterations;
+    m.num_vcycles     = o.num_vcycles;
+    m.coarse_max_iter = o.coarse_max_iterations;
+    m.coarse_rtol     = o.coarse_relative_tolerance;
+    m.coarse_atol     = o.coarse_absolute_tolerance;
+    m.gca             = o.gca;
+    m.fp32            = o.mixed_precision != 0;
+    m.seed            = o.seed;
+    need(o.gca == 0 || o.gca == 1, "gca must be 0 or 1");
+    return m;
+}
+
+// stored packed matrices -> (cells, 2, 18, 18) full symmetric host array
+void unpack_matrices(const tn::EpsDivDivOp& op, double* mats_host)
+{
+    need(op.stored && op.mats.get(), "the operator has no stored matrices");
+    const int64_t       nc = op.lvl().cells();
+    std::vector<double> packed(static_cast<size_t>(tn::gca_values_per_cell()) * nc);
+    tn::cuda_check(cudaMemcpy(packed.data(), op.mats.get(), packed.size() * sizeof(double), cudaMemcpyDeviceToHost),
+                   "copy matrices");
+    for (int64_t c = 0; c < nc; ++c)
+        for (int w = 0; w < 2; ++w) {
+            int p = 0;
+            for (int i = 0; i < 18; ++i)
+                for (int j = i; j < 18; ++j, ++p) {
+                    const double v                             = packed[static_cast<size_t>(w * 171 + p) * nc + c];
+                    mats_host[((c * 2 + w) * 18 + i) * 18 + j] = v;
+                    mats_host[((c * 2 + w) * 18 + j) * 18 + i] = v;
+                }
+        }
 }
 
 tn::EpsDivDivOp* as_edd(tn_operator* op)
@@ -517,6 +560,243 @@ int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void*
         tn::cuda_check(cudaMemcpyAsync(result, red, sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)),
                        "dot readback");
         tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "dot sync");
+    });
+}
+
+
+/* ---- stored matrices and Galerkin coarse operators ---------------------- */
+int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream)
+{
+    return guarded([&] {
+        need(op != nullptr, "NULL operator");
+        need(mode == TN_STORED_OFF || mode == TN_STORED_FULL, "mode must be TN_STORED_OFF or TN_STORED_FULL");
+        auto* e = as_edd(op);
+        if (mode == TN_STORED_OFF) {
+            need(e->k.get() != nullptr, "the operator has no coefficient for the matrix-free mode");
+            e->stored = false;
+            return;
+        }
+        e->set_stored_matrices_from_coefficient(as_stream(stream));
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
+    });
+}
+
+int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream)
+{
+    return guarded([&] {
+        need(fine && coarse, "NULL operator");
+        tn::gca_coarsen(*as_edd(fine), *as_edd(coarse), as_stream(stream));
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
+    });
+}
+
+int tn_operator_copy_local_matrices(tn_operator* op, double* mats_host)
+{
+    return guarded([&] {
+        need(op && mats_host, "NULL argument");
+        unpack_matrices(*as_edd(op), mats_host);
+    });
+}
+
+int tn_vec_random(tn_shell* shell, int level, int precision, int ncomp, uint64_t seed, void* const* comps_dev,
+                  void* stream)
+{
+    return guarded([&] {
+        need(shell && comps_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        precision_size(precision);
+        const auto& L = shell->impl->level(level);
+        int         rc;
+        if (precision == TN_F64)
+            rc = tn::random_fill<double>(L.nodes(), ncomp, reinterpret_cast<double* const*>(comps_dev), L.nr(),
+                                         L.canon_lat.as<int32_t>(), seed, as_stream(stream));
+        else
+            rc = tn::random_fill<float>(L.nodes(), ncomp, reinterpret_cast<float* const*>(comps_dev), L.nr(),
+                                        L.canon_lat.as<int32_t>(), seed, as_stream(stream));
+        if (rc) throw tn::Error(tn::kErrCuda, "random fill launch failed");
+    });
+}
+
+/* ---- solvers ------------------------------------------------------------ */
+void tn_solver_options_default(tn_solver_options* o)
+{
+    if (!o) return;
+    o->restart                   = 30;
+    o->max_iterations            = 300;
+    o->relative_tolerance        = 1e-8;
+    o->absolute_tolerance        = 1e-12;
+    o->chebyshev_order           = 2;
+    o->chebyshev_iterations      = 2;
+    o->power_iterations          = 10;
+    o->num_vcycles               = 1;
+    o->coarse_max_iterations     = 50;
+    o->coarse_relative_tolerance = 1e-6;
+    o->coarse_absolute_tolerance = 1e-16;
+    o->gca                       = 1;
+    o->mixed_precision           = 0;
+    o->seed                      = 12345;
+    o->normalize_pressure        = 1;
+}
+
+int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,
+                            const double* eta_cell_dev, const double* k_schur_dev, int bc_cmb, int bc_surface,
+                            const tn_solver_options* opts, void* stream, tn_solver** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        check_bcs(bc_cmb, bc_surface);
+        tn_solver_options o;
+        tn_solver_options_default(&o);
+        if (opts) o = *opts;
+        tn::StokesOptions so;
+        so.restart  = o.restart;
+        so.max_iter = o.max_iterations;
+        so.rtol     = o.relative_tolerance;
+        so.atol     = o.absolute_tolerance;
+        so.mg       = mg_options(o);
+        so.normalize_pressure = o.normalize_pressure != 0;
+        auto s      = std::make_unique<tn_solver>();
+        s->shell    = shell;
+        s->stokes   = std::make_unique<tn::StokesSolver>(shell->impl.get(), velocity_level, eta_nodal_dev,
+                                                       eta_cell_dev, k_schur_dev, bc_cmb, bc_surface, so,
+                                                       as_stream(stream));
+        *out = s.release();
+    });
+}
+
+int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+                              int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
+                              tn_solver** out)
+{
+    return guarded([&] {
+        need(shell && out, "NULL argument");
+        check_bcs(bc_cmb, bc_surface);
+        tn_solver_options o;
+        tn_solver_options_default(&o);
+        if (opts) o = *opts;
+        tn::VelocitySolverOptions vo;
+        vo.max_iter = o.max_iterations;
+        vo.rtol     = o.relative_tolerance;
+        vo.atol     = o.absolute_tolerance;
+        vo.mg       = mg_options(o);
+        auto s      = std::make_unique<tn_solver>();
+        s->shell    = shell;
+        s->velocity = std::make_unique<tn::VelocitySolver>(shell->impl.get(), level, eta_nodal_dev, eta_cell_dev,
+                                                           bc_cmb, bc_surface, vo, as_stream(stream));
+        *out = s.release();
+    });
+}
+
+void tn_solver_destroy(tn_solver* s) { delete s; }
+
+int tn_solver_solve(tn_solver* s, double* const* x_dev, const double* const* b_dev, void* stream)
+{
+    int converged = 0;
+    const int rc  = guarded([&] {
+        need(s && x_dev && b_dev, "NULL argument");
+        if (s->stokes) {
+            const double* fu[3] = {b_dev[0], b_dev[1], b_dev[2]};
+            double*       u[3]  = {x_dev[0], x_dev[1], x_dev[2]};
+            converged           = s->stokes->solve(u, x_dev[3], fu, b_dev[3], as_stream(stream));
+        } else {
+            converged = s->velocity->solve(x_dev, b_dev, as_stream(stream));
+        }
+    });
+    if (rc != TN_OK) return rc;
+    if (!converged) {
+        g_last_error = "the solver stopped before reaching its tolerance";
+        return TN_ERR_NOT_CONVERGED;
+    }
+    return TN_OK;
+}
+
+int tn_solver_result(const tn_solver* s, int* iterations, double* relative_residual, int* converged)
+{
+    return guarded([&] {
+        need(s != nullptr, "NULL solver");
+        const int    it = s->stokes ? s->stokes->iterations : s->velocity->iterations;
+        const double rr = s->stokes ? s->stokes->final_relres : s->velocity->final_relres;
+        const bool   cv = s->stokes ? s->stokes->converged : s->velocity->converged;
+        if (iterations) *iterations = it;
+        if (relative_residual) *relative_residual = rr;
+        if (converged) *converged = cv ? 1 : 0;
+    });
+}
+
+int tn_solver_history(const tn_solver* s, double* history_host, int capacity, int* length)
+{
+    return guarded([&] {
+        need(s && length, "NULL argument");
+        const auto& h = s->stokes ? s->stokes->history : s->velocity->history;
+        *length       = static_cast<int>(h.size());
+        if (history_host)
+            for (int i = 0; i < capacity && i < static_cast<int>(h.size()); ++i) history_host[i] = h[i];
+    });
+}
+
+int tn_solver_precondition(tn_solver* s, const double* const* v_dev, double* const* z_dev, void* stream)
+{
+    return guarded([&] {
+        need(s && v_dev && z_dev, "NULL argument");
+        if (s->stokes)
+            s->stokes->precondition_external(v_dev, z_dev, as_stream(stream));
+        else
+            s->velocity->precondition_external(v_dev, z_dev, as_stream(stream));
+    });
+}
+
+int tn_solver_vcycle(tn_solver* s, int precision, void* const* x_dev, const void* const* b_dev, void* stream)
+{
+    return guarded([&] {
+        need(s && x_dev && b_dev, "NULL argument");
+        precision_size(precision);
+        if (precision == TN_F64)
+            s->mg().solve_external<double>(reinterpret_cast<double* const*>(x_dev),
+                                           reinterpret_cast<const double* const*>(b_dev), as_stream(stream));
+        else
+            s->mg().solve_external<float>(reinterpret_cast<float* const*>(x_dev),
+                                          reinterpret_cast<const float* const*>(b_dev), as_stream(stream));
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
+    });
+}
+
+int tn_solver_level_lambda(tn_solver* s, int level, double* lambda_max)
+{
+    return guarded([&] {
+        need(s && lambda_max, "NULL argument");
+        need(level >= 1 && level <= s->mg().fine_level(), "level must be in 1..fine level");
+        *lambda_max = s->mg().lambda(level);
+    });
+}
+
+int tn_solver_inverse_diagonal(tn_solver* s, int level, double* const* out_dev, void* stream)
+{
+    return guarded([&] {
+        need(s && out_dev, "NULL argument");
+        need(level >= 1 && level <= s->mg().fine_level(), "level must be in 1..fine level");
+        const auto& d = s->mg().inv_diag(level);
+        for (int c = 0; c < 3; ++c)
+            tn::cuda_check(cudaMemcpyAsync(out_dev[c], d.comp(0, c), sizeof(double) * d.d.seg[0].n,
+                                           cudaMemcpyDeviceToDevice, as_stream(stream)),
+                           "copy");
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
+    });
+}
+
+int tn_solver_coarse_stats(tn_solver* s, double* stats3)
+{
+    return guarded([&] {
+        need(s && stats3, "NULL argument");
+        s->mg().coarse_stats(stats3, nullptr);
+    });
+}
+
+int tn_solver_level_matrices(tn_solver* s, int level, double* mats_host)
+{
+    return guarded([&] {
+        need(s && mats_host, "NULL argument");
+        need(level >= 0 && level < s->mg().fine_level(), "level must be a coarse level");
+        unpack_matrices(s->mg().op64(level), mats_host);
     });
 }
 

@@ -1,5 +1,8 @@
 // Host runtime: device mesh construction and operator dispatch.
+#include <algorithm>
 #include <cstring>
+
+#include <type_traits>
 
 #include "tn_runtime.hpp"
 
@@ -36,6 +39,16 @@ std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, 
         dl->owned_lat         = upload(h.owned_lat);
         dl->dup_offset        = upload(h.dup_offset);
         dl->dup_members       = upload(h.dup_members);
+        {
+            std::vector<int32_t> canon(h.owned_lat.size());
+            for (size_t i = 0; i < canon.size(); ++i) canon[i] = static_cast<int32_t>(i);
+            for (size_t c = 0; c + 1 < h.dup_offset.size(); ++c) {
+                int32_t lo = h.dup_members[h.dup_offset[c]];
+                for (int32_t m = h.dup_offset[c]; m < h.dup_offset[c + 1]; ++m) lo = std::min(lo, h.dup_members[m]);
+                for (int32_t m = h.dup_offset[c]; m < h.dup_offset[c + 1]; ++m) canon[h.dup_members[m]] = lo;
+            }
+            dl->canon_lat = upload(canon);
+        }
         dl->iface.num_classes = static_cast<int>(h.dup_offset.size()) - 1;
         dl->iface.offset      = dl->dup_offset.as<int32_t>();
         dl->iface.members     = dl->dup_members.as<int32_t>();
@@ -69,11 +82,92 @@ void iface(const DeviceLevel& L, int ncomp, T* const* v, cudaStream_t st)
 }
 }  // namespace
 
-template <typename T>
-void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st) const
+int64_t EpsDivDivOp::mats_values() const { return static_cast<int64_t>(gca_values_per_cell()) * lvl().cells(); }
+
+void EpsDivDivOp::set_stored_matrices_from_coefficient(cudaStream_t st)
 {
     const DeviceLevel& L = lvl();
-    EddLaunch<T>       p;
+    if (precision != 0) throw Error(kErrUnsupported, "stored matrices are assembled from an FP64 coefficient");
+    if (k.get() == nullptr) throw Error(kErrState, "operator has no coefficient to assemble matrices from");
+    mats.alloc(static_cast<size_t>(mats_values()) * sizeof(double));
+    if (element_matrices(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), q0 ? nullptr : k.as<double>(),
+                         q0 ? k.as<double>() : nullptr, mats.as<double>(), st) != 0)
+        throw Error(kErrCuda, "element matrix assembly launch failed");
+    stored        = true;
+    baked_bc[0]   = -1;
+    baked32_valid = false;
+}
+
+void EpsDivDivOp::ensure_baked(bool need32, cudaStream_t st)
+{
+    const DeviceLevel& L = lvl();
+    if (!stored || mats.get() == nullptr) throw Error(kErrState, "stored matrix mode without matrices");
+    const size_t nv = static_cast<size_t>(mats_values());
+    if (baked_bc[0] != bc_cmb || baked_bc[1] != bc_surf || baked64.get() == nullptr) {
+        if (baked64.get() == nullptr) baked64.alloc(nv * sizeof(double));
+        cuda_check(cudaMemcpyAsync(baked64.get(), mats.get(), nv * sizeof(double), cudaMemcpyDeviceToDevice, st),
+                   "copy matrices");
+        if (gca_bake_boundary(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), bc_cmb, bc_surf,
+                              baked64.as<double>(), st) != 0)
+            throw Error(kErrCuda, "boundary bake launch failed");
+        baked_bc[0]   = bc_cmb;
+        baked_bc[1]   = bc_surf;
+        baked32_valid = false;
+    }
+    if (need32 && !baked32_valid) {
+        if (baked32.get() == nullptr) baked32.alloc(nv * sizeof(float));
+        if (gca_to_f32(static_cast<int64_t>(nv), baked64.as<double>(), baked32.as<float>(), st) != 0)
+            throw Error(kErrCuda, "matrix conversion launch failed");
+        baked32_valid = true;
+    }
+}
+
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st)
+{
+    if (fine.shell != coarse.shell || coarse.level != fine.level - 1)
+        throw Error(kErrArg, "GCA needs operators on consecutive levels of one shell");
+    const DeviceLevel& Lf = fine.lvl();
+    if (!fine.stored && (fine.precision != 0 || fine.k.get() == nullptr))
+        throw Error(kErrUnsupported, "GCA needs an FP64 fine coefficient or stored fine matrices");
+    coarse.mats.alloc(static_cast<size_t>(coarse.mats_values()) * sizeof(double));
+    const double* kf   = (!fine.stored && !fine.q0) ? fine.k.as<double>() : nullptr;
+    const double* kq0f = (!fine.stored && fine.q0) ? fine.k.as<double>() : nullptr;
+    if (gca_build(Lf.nl(), Lf.nr(), Lf.coords<double>(), Lf.radii<double>(), kf, kq0f,
+                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st) != 0)
+        throw Error(kErrCuda, "GCA build launch failed");
+    coarse.stored        = true;
+    coarse.baked_bc[0]   = -1;
+    coarse.baked32_valid = false;
+}
+
+template <typename T>
+void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
+{
+    const DeviceLevel& L = lvl();
+    for (int c = 0; c < 3; ++c) {
+        check_aligned<T>(src[c]);
+        check_aligned<T>(dst[c]);
+    }
+    if (stored) {
+        if (apply_mode == 0) zero_components<T>(L.nodes(), 3, dst, st);
+        if (diagonal) {
+            if (!std::is_same<T, double>::value)
+                throw Error(kErrUnsupported, "diagonal mode of a stored operator is FP64 only");
+            if (gca_diag_add(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), bc_cmb, bc_surf,
+                             mats.as<double>(), reinterpret_cast<const double* const*>(src),
+                             reinterpret_cast<double* const*>(dst), st) != 0)
+                throw Error(kErrCuda, "stored diagonal launch failed");
+        } else {
+            ensure_baked(std::is_same<T, float>::value, st);
+            const T* m = std::is_same<T, float>::value ? static_cast<const T*>(baked32.get())
+                                                       : static_cast<const T*>(baked64.get());
+            if (gca_apply_add<T>(L.nl(), L.nr(), m, src, dst, st) != 0)
+                throw Error(kErrCuda, "stored apply launch failed");
+        }
+        if (comm_mode == 1) iface<T>(L, 3, dst, st);
+        return;
+    }
+    EddLaunch<T> p;
     p.nl     = L.nl();
     p.nr     = L.nr();
     p.coords = L.coords<T>();
@@ -85,8 +179,6 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st) c
     for (int c = 0; c < 3; ++c) {
         p.src[c] = src[c];
         p.dst[c] = dst[c];
-        check_aligned<T>(src[c]);
-        check_aligned<T>(dst[c]);
     }
     p.bc_cmb   = bc_cmb;
     p.bc_surf  = bc_surf;
@@ -99,6 +191,8 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st) c
     if (rc != 0) throw Error(kErrCuda, "epsdivdiv launch failed (" + std::to_string(rc) + ")");
     if (comm_mode == 1) iface<T>(L, 3, dst, st);
 }
+template void EpsDivDivOp::apply_t<double>(const double* const*, double* const*, cudaStream_t);
+template void EpsDivDivOp::apply_t<float>(const float* const*, float* const*, cudaStream_t);
 
 void EpsDivDivOp::apply(void* const* src, void* const* dst, cudaStream_t st)
 {

@@ -1,0 +1,721 @@
+// Kernels of the Krylov / multigrid solver layer.
+//
+// * Owned-node dot products over (block) vectors laid out as segments of
+//   components (velocity on level L, pressure on level L-1), reduced in a fixed
+//   order by the last block to finish (no second launch, bitwise reproducible),
+//   with the result left in device memory so that the host does not wait.
+// * The FGMRES modified Gram-Schmidt step fused into one pass: w -= h_{i-1}
+//   v_{i-1} followed by h_i = <w, v_i> (fgmres.hpp:230-240 does the same
+//   arithmetic as two launches per basis vector, dot then lincomb).
+// * The Chebyshev-Jacobi update d = alpha D^-1 (b - A x) + beta d, x += d in one
+//   pass (chebyshev.hpp:102-176 uses four BLAS-1 launches per step).
+// * The coarsest-grid CG (pcg.hpp:81-169, identity preconditioner) as a single
+//   thread-block-cluster kernel over stored element matrices: the CTAs of one
+//   cluster synchronise with the hardware cluster barrier, so the whole solve is
+//   one launch.
+#include <cfloat>
+
+#include "tn_device.cuh"
+#include "tn_kernels.hpp"
+
+namespace tn {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBlocks  = 592;  // 4 x 148 SMs
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block sum, then the last block of the grid sums the per-block partials in
+// index order and writes *out (sqrt of it when take_sqrt).
+__device__ void block_finish(double v, RedScratch rs, double* out, int take_sqrt)
+{
+    __shared__ double red[kThreads / 32];
+    __shared__ int    is_last;
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) s += red[k];
+        rs.partials[blockIdx.x] = s;
+        __threadfence();
+        const unsigned t = atomicAdd(rs.counter, 1u);
+        is_last          = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        double s = 0.0;
+        for (int k = threadIdx.x; k < static_cast<int>(gridDim.x); k += blockDim.x) s += __ldcg(rs.partials + k);
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int k = 0; k < kThreads / 32; ++k) tot += red[k];
+            *out        = take_sqrt ? sqrt(tot) : tot;
+            *rs.counter = 0u;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) vdot_kernel(VecDesc L, const T* __restrict__ a, const T* __restrict__ b,
+                                                         RedScratch rs, double* out, int take_sqrt)
+{
+    double        acc    = 0.0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int s = 0; s < L.nseg; ++s) {
+        const VecSeg   S  = L.seg[s];
+        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        for (int c = 0; c < S.ncomp; ++c) {
+            const T* pa = a + S.offset + c * S.stride;
+            const T* pb = b + S.offset + c * S.stride;
+            for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride)
+                if (S.owned[static_cast<uint32_t>(i) / nr])
+                    acc += static_cast<double>(pa[i]) * static_cast<double>(pb[i]);
+        }
+    }
+    block_finish(acc, rs, out, take_sqrt);
+}
+
+__global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __restrict__ w,
+                                                        const double* __restrict__ vsub, const double* hsub,
+                                                        const double* __restrict__ vdot, RedScratch rs, double* out,
+                                                        int take_sqrt)
+{
+    const double  h      = vsub ? *hsub : 0.0;
+    double        acc    = 0.0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int s = 0; s < L.nseg; ++s) {
+        const VecSeg   S  = L.seg[s];
+        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        for (int c = 0; c < S.ncomp; ++c) {
+            const int64_t o = S.offset + c * S.stride;
+            for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride) {
+                double wi = w[o + i];
+                if (vsub) {
+                    wi        = wi - h * vsub[o + i];
+                    w[o + i]  = wi;
+                }
+                if (S.owned[static_cast<uint32_t>(i) / nr]) acc += wi * (vdot ? vdot[o + i] : wi);
+            }
+        }
+    }
+    block_finish(acc, rs, out, take_sqrt);
+}
+
+// CG update x += alpha p, r -= alpha ap with alpha = s_an / s_ad from device
+// memory, then *out = ||r|| (owned). Skips the update when |s_ad| < DBL_MIN
+// (pcg.hpp:119-124 returns there) and writes *out = -1 so the host can tell.
+__global__ void __launch_bounds__(kThreads) cg_update_kernel(VecDesc L, double* __restrict__ x,
+                                                              double* __restrict__ r, const double* __restrict__ p,
+                                                              const double* __restrict__ ap, const double* s_an,
+                                                              const double* s_ad, RedScratch rs, double* out)
+{
+    const double ad = *s_ad;
+    if (fabs(ad) < DBL_MIN) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out = -1.0;
+        return;
+    }
+    const double  alpha  = *s_an / ad;
+    double        acc    = 0.0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int s = 0; s < L.nseg; ++s) {
+        const VecSeg   S  = L.seg[s];
+        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        for (int c = 0; c < S.ncomp; ++c) {
+            const int64_t o = S.offset + c * S.stride;
+            for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride) {
+                x[o + i]        = x[o + i] + alpha * p[o + i];
+                const double rv = r[o + i] - alpha * ap[o + i];
+                r[o + i]        = rv;
+                if (S.owned[static_cast<uint32_t>(i) / nr]) acc += rv * rv;
+            }
+        }
+    }
+    block_finish(acc, rs, out, 1);
+}
+
+// p = z + (s_num / s_den) p
+__global__ void p_update_kernel(int64_t n, double* __restrict__ p, const double* __restrict__ z, const double* s_num,
+                                const double* s_den)
+{
+    const double  beta   = *s_num / *s_den;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        p[i] = z[i] + beta * p[i];
+}
+
+template <typename T>
+__global__ void scale_recip_kernel(int64_t n, T* __restrict__ y, const T* __restrict__ x, const double* s)
+{
+    const T       f      = static_cast<T>(1.0 / *s);
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = f * x[i];
+}
+
+template <typename T, bool FIRST>
+__global__ void cheb_kernel(int64_t n, T* __restrict__ x, T* __restrict__ d, const T* __restrict__ b,
+                            const T* __restrict__ ax, const T* __restrict__ invd, T alpha, T beta)
+{
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const T z  = (b[i] - ax[i]) * invd[i];
+        const T dn = FIRST ? alpha * z : alpha * z + beta * d[i];
+        d[i]       = dn;
+        x[i]       = x[i] + dn;
+    }
+}
+
+template <typename T>
+__global__ void mul_kernel(int64_t n, T* __restrict__ y, const T* __restrict__ a, const T* __restrict__ b, T c)
+{
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        y[i] = c * (a[i] * b[i]);
+}
+
+__global__ void multi_axpy_kernel(int64_t n, double* __restrict__ x, AxpyList L)
+{
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double acc = 0.0;
+        for (int k = 0; k < L.m; ++k) acc = acc + L.y[k] * L.z[k][i];
+        x[i] = x[i] + acc;
+    }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+struct CompPtrs {
+    T* p[4];
+};
+
+template <typename T>
+__global__ void random_kernel(int64_t n, int ncomp, CompPtrs<T> v, int nr, const int32_t* __restrict__ canon_lat,
+                              uint64_t seed)
+{
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int c = 0; c < ncomp; ++c)
+        for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const uint64_t lat = static_cast<uint64_t>(i / nr), r = static_cast<uint64_t>(i % nr);
+            const uint64_t gid = (static_cast<uint64_t>(canon_lat[lat]) * nr + r) * ncomp + c;
+            const uint64_t z   = splitmix64(seed + (gid + 1) * 0x9E3779B97F4A7C15ull);
+            const double   u   = static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0);
+            v.p[c][i]          = static_cast<T>(2.0 * u - 1.0);
+        }
+}
+
+template <typename T>
+__global__ void nonfinite_kernel(int64_t n, const T* __restrict__ a, int* flag)
+{
+    bool          bad    = false;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (!isfinite(static_cast<double>(a[i]))) bad = true;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 1);
+}
+
+// f32 -> f64 with a non-finite flag (the FGMRES NaN/Inf check of the
+// preconditioner output, fgmres.hpp:191-210, folded into the conversion).
+__global__ void widen_check_kernel(int64_t n, const float* __restrict__ in, double* __restrict__ out, int* flag)
+{
+    bool          bad    = false;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double v = static_cast<double>(in[i]);
+        if (!isfinite(v)) bad = true;
+        out[i] = v;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest-grid CG in one cluster launch.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int woff_c(int w, int n, int k)
+{
+    constexpr int t[2][6][3] = {{{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}},
+                                {{1, 1, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 1}, {0, 1, 1}, {1, 0, 1}}};
+    return t[w][n][k];
+}
+__device__ __forceinline__ int pidx18(int i, int j)
+{
+    if (i > j) {
+        const int t = i;
+        i           = j;
+        j           = t;
+    }
+    return i * (36 - i + 1) / 2 + (j - i);
+}
+
+// Cluster-wide barrier; release / acquire at cluster scope orders the global
+// memory accesses of all threads of the cluster around it.
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_ncta()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+constexpr int kPcgThreads = 1024;
+constexpr int kPcgMaxCta  = 16;
+
+// Sum of v over the cluster; every thread returns the same value (partials are
+// summed in rank order).
+__device__ double cluster_sum(double v, double* partials, int& buf, unsigned rank, unsigned ncta, double* red)
+{
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < kPcgThreads / 32; ++k) s += red[k];
+        partials[buf * kPcgMaxCta + rank] = s;
+    }
+    cluster_barrier();
+    double tot = 0.0;
+    for (unsigned k = 0; k < ncta; ++k) tot += __ldcg(partials + buf * kPcgMaxCta + k);
+    buf ^= 1;
+    return tot;
+}
+
+// Per-CTA view of the coarsest level: this CTA's cells [c0, c0 + cnt), their
+// node indices (int32, [w * 6 + n][local cell]) and their matrices (packed
+// value-major, in shared memory when they fit, else the global array).
+struct PcgView {
+    int            c0, cnt, cpc;
+    const int32_t* node;  // shared, [12][cpc]
+    const double*  mb;    // matrices of local cell lc at mb[p * ms + lc]
+    int64_t        ms;
+};
+
+__device__ __forceinline__ int pidx_rt(int a, int b)
+{
+    const int i = a < b ? a : b, j = a < b ? b : a;
+    return i * (37 - i) / 2 + (j - i);
+}
+
+// dst (zero on entry) = A src with the interface sum; ends with a cluster barrier.
+__device__ void pcg_matvec(const CoarsePcgArgs& A, const PcgView& V, const double* src, double* dst, unsigned g,
+                           unsigned G)
+{
+    const int64_t S     = A.stride;
+    const int     items = 36 * V.cnt;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int lc   = it % V.cnt;
+        const int rest = it / V.cnt;
+        const int w    = rest & 1;
+        const int a    = rest >> 1;
+        double    acc  = 0.0;
+#pragma unroll
+        for (int b = 0; b < 18; ++b) {
+            const int nb = b % 6, cb = b / 6;
+            acc += V.mb[static_cast<int64_t>(w * 171 + pidx_rt(a, b)) * V.ms + lc] *
+                   __ldcg(src + cb * S + V.node[(w * 6 + nb) * V.cpc + lc]);
+        }
+        const int na = a % 6, ca = a / 6;
+        atomicAdd(dst + ca * S + V.node[(w * 6 + na) * V.cpc + lc], acc);
+    }
+    cluster_barrier();
+    const int nr     = A.nr;
+    const int iitems = A.num_classes * nr * 3;
+    for (int it = static_cast<int>(g); it < iitems; it += static_cast<int>(G)) {
+        const int r    = it % nr;
+        const int rest = it / nr;
+        const int c    = rest % 3;
+        const int cls  = rest / 3;
+        const int b0 = A.off[cls], b1 = A.off[cls + 1];
+        double*   v  = dst + c * S;
+        double    s  = 0.0;
+        for (int m = b0; m < b1; ++m) s += __ldcg(v + static_cast<int64_t>(A.mem[m]) * nr + r);
+        for (int m = b0; m < b1; ++m) v[static_cast<int64_t>(A.mem[m]) * nr + r] = s;
+    }
+    cluster_barrier();
+}
+
+__global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_kernel(CoarsePcgArgs A)
+{
+    extern __shared__ __align__(16) unsigned char pcg_smem[];
+    __shared__ double red[kPcgThreads / 32];
+    const unsigned    rank = cluster_rank(), ncta = cluster_ncta();
+    const unsigned    g = rank * kPcgThreads + threadIdx.x, G = ncta * kPcgThreads;
+    const int         nl = A.nl, nr = A.nr;
+    const int         nc = 10 * (nl - 1) * (nl - 1) * (nr - 1);
+
+    PcgView V;
+    V.cpc = A.cells_per_cta;
+    V.c0  = static_cast<int>(rank) * V.cpc;
+    V.cnt = nc - V.c0 < V.cpc ? nc - V.c0 : V.cpc;
+    if (V.cnt < 0) V.cnt = 0;
+    int32_t* node = reinterpret_cast<int32_t*>(pcg_smem);
+    for (int i = threadIdx.x; i < 12 * V.cpc; i += blockDim.x) {
+        const int lc = i % V.cpc, k = i / V.cpc;
+        int32_t   v  = 0;
+        if (lc < V.cnt) {
+            const int cell = V.c0 + lc;
+            const int r    = cell % (nr - 1);
+            int       t    = cell / (nr - 1);
+            const int y    = t % (nl - 1);
+            t /= (nl - 1);
+            const int x = t % (nl - 1), d = t / (nl - 1);
+            const int w = k / 6, n = k % 6;
+            v = static_cast<int32_t>(
+                node_index(nl, nr, d, x + woff_c(w, n, 0), y + woff_c(w, n, 1), r + woff_c(w, n, 2)));
+        }
+        node[i] = v;
+    }
+    V.node = node;
+    if (A.mats_in_smem) {
+        double* ms = reinterpret_cast<double*>(pcg_smem + A.node_bytes);
+        for (int i = threadIdx.x; i < 342 * V.cpc; i += blockDim.x) {
+            const int lc = i % V.cpc, p = i / V.cpc;
+            ms[i]        = lc < V.cnt ? A.mats[static_cast<int64_t>(p) * nc + V.c0 + lc] : 0.0;
+        }
+        V.mb = ms;
+        V.ms = V.cpc;
+    } else {
+        V.mb = A.mats + V.c0;
+        V.ms = nc;
+    }
+    __syncthreads();
+
+    const int      n = static_cast<int>(A.n), n3 = 3 * n;
+    const int64_t  S = A.stride;
+    const uint32_t unr = static_cast<uint32_t>(nr);
+    int            buf = 0;
+    for (int i = static_cast<int>(g); i < n3; i += static_cast<int>(G)) {
+        const int c = i / n, j = i - c * n;
+        A.ap[c * S + j] = 0.0;
+    }
+    cluster_barrier();
+    pcg_matvec(A, V, A.x, A.ap, g, G);
+    double acc = 0.0;
+    for (int i = static_cast<int>(g); i < n3; i += static_cast<int>(G)) {
+        const int     c = i / n, j = i - c * n;
+        const int64_t o = c * S + j;
+        const double  rv = __ldcg(A.b + o) - __ldcg(A.ap + o);
+        A.r[o]           = rv;
+        A.p[o]           = rv;
+        A.ap[o]          = 0.0;
+        if (A.owned[static_cast<uint32_t>(j) / unr]) acc += rv * rv;
+    }
+    double       rr   = cluster_sum(acc, A.partials, buf, rank, ncta, red);
+    const double init = sqrt(rr);
+    double       res  = init;
+    int          its  = 0;
+    if (!(init < A.atol)) {
+        double an = rr;
+        for (int it = 1; it <= A.max_iter; ++it) {
+            pcg_matvec(A, V, A.p, A.ap, g, G);
+            acc = 0.0;
+            for (int i = static_cast<int>(g); i < n3; i += static_cast<int>(G)) {
+                const int     c = i / n, j = i - c * n;
+                const int64_t o = c * S + j;
+                if (A.owned[static_cast<uint32_t>(j) / unr]) acc += __ldcg(A.ap + o) * __ldcg(A.p + o);
+            }
+            const double ad = cluster_sum(acc, A.partials, buf, rank, ncta, red);
+            if (fabs(ad) < DBL_MIN) break;
+            const double alpha = an / ad;
+            acc                = 0.0;
+            for (int i = static_cast<int>(g); i < n3; i += static_cast<int>(G)) {
+                const int     c = i / n, j = i - c * n;
+                const int64_t o = c * S + j;
+                A.x[o]          = __ldcg(A.x + o) + alpha * __ldcg(A.p + o);
+                const double rv = __ldcg(A.r + o) - alpha * __ldcg(A.ap + o);
+                A.r[o]          = rv;
+                if (A.owned[static_cast<uint32_t>(j) / unr]) acc += rv * rv;
+            }
+            rr  = cluster_sum(acc, A.partials, buf, rank, ncta, red);
+            res = sqrt(rr);
+            its = it;
+            if (res / init <= A.rtol || res < A.atol) break;
+            const double bn = rr;
+            if (fabs(an) < DBL_MIN) break;
+            const double beta = bn / an;
+            for (int i = static_cast<int>(g); i < n3; i += static_cast<int>(G)) {
+                const int     c = i / n, j = i - c * n;
+                const int64_t o = c * S + j;
+                A.p[o]          = __ldcg(A.r + o) + beta * __ldcg(A.p + o);
+                A.ap[o]         = 0.0;
+            }
+            cluster_barrier();
+            an = bn;
+        }
+    }
+    if (g == 0 && A.stats) {
+        A.stats[0] = static_cast<double>(its);
+        A.stats[1] = init;
+        A.stats[2] = res;
+    }
+}
+
+__global__ void inject_kernel(int nlc, int nrc, const double* __restrict__ fine, double* __restrict__ coarse,
+                              int reciprocal)
+{
+    const int     nlf = 2 * nlc - 1, nrf = 2 * nrc - 1;
+    const int64_t n   = 10ll * nlc * nlc * nrc;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int r = static_cast<int>(i % nrc);
+        int64_t   t = i / nrc;
+        const int y = static_cast<int>(t % nlc);
+        t /= nlc;
+        const int    x = static_cast<int>(t % nlc);
+        const int    d = static_cast<int>(t / nlc);
+        const double v = fine[node_index(nlf, nrf, d, 2 * x, 2 * y, 2 * r)];
+        coarse[i]      = reciprocal ? 1.0 / v : v;
+    }
+}
+
+__global__ void cell_average_kernel(int nlc, int nrc, const double* __restrict__ fine, double* __restrict__ coarse)
+{
+    const int     nlf = 2 * nlc - 1, nrf = 2 * nrc - 1;
+    const int64_t n   = 10ll * (nlc - 1) * (nlc - 1) * (nrc - 1);
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int r = static_cast<int>(i % (nrc - 1));
+        int64_t   t = i / (nrc - 1);
+        const int y = static_cast<int>(t % (nlc - 1));
+        t /= (nlc - 1);
+        const int x = static_cast<int>(t % (nlc - 1));
+        const int d = static_cast<int>(t / (nlc - 1));
+        double    s = 0.0;
+        for (int c = 0; c < 8; ++c)
+            s += fine[node_index(nlf - 1, nrf - 1, d, 2 * x + (c & 1), 2 * y + ((c >> 1) & 1), 2 * r + (c >> 2))];
+        coarse[i] = 0.125 * s;
+    }
+}
+
+inline int grid_for(int64_t n)
+{
+    int64_t b = (n + kThreads - 1) / kThreads;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return static_cast<int>(b);
+}
+inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+
+}  // namespace
+
+int solver_partials_size() { return kBlocks; }
+
+template <typename T>
+int vec_dot(const VecDesc& L, const T* a, const T* b, double* out_dev, RedScratch rs, bool take_sqrt, cudaStream_t st)
+{
+    vdot_kernel<T><<<kBlocks, kThreads, 0, st>>>(L, a, b, rs, out_dev, take_sqrt ? 1 : 0);
+    return launch_status();
+}
+template int vec_dot<double>(const VecDesc&, const double*, const double*, double*, RedScratch, bool, cudaStream_t);
+template int vec_dot<float>(const VecDesc&, const float*, const float*, double*, RedScratch, bool, cudaStream_t);
+
+int mgs_step(const VecDesc& L, double* w, const double* v_sub, const double* h_sub, const double* v_dot, double* out,
+             RedScratch rs, cudaStream_t st)
+{
+    mgs_kernel<<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, v_dot ? 0 : 1);
+    return launch_status();
+}
+
+int cg_update(const VecDesc& L, double* x, double* r, const double* p, const double* ap, const double* s_an,
+              const double* s_ad, double* out, RedScratch rs, cudaStream_t st)
+{
+    cg_update_kernel<<<kBlocks, kThreads, 0, st>>>(L, x, r, p, ap, s_an, s_ad, rs, out);
+    return launch_status();
+}
+
+int p_update(int64_t n, double* p, const double* z, const double* s_num, const double* s_den, cudaStream_t st)
+{
+    p_update_kernel<<<grid_for(n), kThreads, 0, st>>>(n, p, z, s_num, s_den);
+    return launch_status();
+}
+
+template <typename T>
+int scale_by_recip(int64_t n, T* y, const T* x, const double* s_dev, cudaStream_t st)
+{
+    scale_recip_kernel<T><<<grid_for(n), kThreads, 0, st>>>(n, y, x, s_dev);
+    return launch_status();
+}
+template int scale_by_recip<double>(int64_t, double*, const double*, const double*, cudaStream_t);
+template int scale_by_recip<float>(int64_t, float*, const float*, const double*, cudaStream_t);
+
+template <typename T>
+int cheb_step(int64_t n, T* x, T* d, const T* b, const T* ax, const T* invdiag, T alpha, T beta, bool first,
+              cudaStream_t st)
+{
+    if (first)
+        cheb_kernel<T, true><<<grid_for(n), kThreads, 0, st>>>(n, x, d, b, ax, invdiag, alpha, beta);
+    else
+        cheb_kernel<T, false><<<grid_for(n), kThreads, 0, st>>>(n, x, d, b, ax, invdiag, alpha, beta);
+    return launch_status();
+}
+template int cheb_step<double>(int64_t, double*, double*, const double*, const double*, const double*, double, double,
+                               bool, cudaStream_t);
+template int cheb_step<float>(int64_t, float*, float*, const float*, const float*, const float*, float, float, bool,
+                              cudaStream_t);
+
+template <typename T>
+int vec_mul(int64_t n, T* y, const T* a, const T* b, T c, cudaStream_t st)
+{
+    mul_kernel<T><<<grid_for(n), kThreads, 0, st>>>(n, y, a, b, c);
+    return launch_status();
+}
+template int vec_mul<double>(int64_t, double*, const double*, const double*, double, cudaStream_t);
+template int vec_mul<float>(int64_t, float*, const float*, const float*, float, cudaStream_t);
+
+int multi_axpy(int64_t n, double* x, const AxpyList& list, cudaStream_t st)
+{
+    if (list.m < 0 || list.m > kMaxAxpy) return -1;
+    if (list.m == 0) return 0;
+    multi_axpy_kernel<<<grid_for(n), kThreads, 0, st>>>(n, x, list);
+    return launch_status();
+}
+
+template <typename T>
+int random_fill(int64_t n, int ncomp, T* const* comps, int nr, const int32_t* canon_lat, uint64_t seed,
+                cudaStream_t st)
+{
+    if (ncomp < 1 || ncomp > 4) return -1;
+    CompPtrs<T> v{};
+    for (int c = 0; c < ncomp; ++c) v.p[c] = comps[c];
+    random_kernel<T><<<grid_for(n), kThreads, 0, st>>>(n, ncomp, v, nr, canon_lat, seed);
+    return launch_status();
+}
+template int random_fill<double>(int64_t, int, double* const*, int, const int32_t*, uint64_t, cudaStream_t);
+template int random_fill<float>(int64_t, int, float* const*, int, const int32_t*, uint64_t, cudaStream_t);
+
+template <typename T>
+int flag_nonfinite(int64_t n, const T* a, int* flag_dev, cudaStream_t st)
+{
+    nonfinite_kernel<T><<<grid_for(n), kThreads, 0, st>>>(n, a, flag_dev);
+    return launch_status();
+}
+template int flag_nonfinite<double>(int64_t, const double*, int*, cudaStream_t);
+template int flag_nonfinite<float>(int64_t, const float*, int*, cudaStream_t);
+
+int widen_check(int64_t n, const float* in, double* out, int* flag_dev, cudaStream_t st)
+{
+    widen_check_kernel<<<grid_for(n), kThreads, 0, st>>>(n, in, out, flag_dev);
+    return launch_status();
+}
+
+namespace {
+// cluster size (16 when the device allows non-portable clusters of this
+// kernel with the given shared memory, else 8)
+int pcg_cluster_size(size_t smem)
+{
+    int size = 8;
+    if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id               = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kPcgMaxCta;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim            = dim3(kPcgMaxCta);
+        cfg.blockDim           = dim3(kPcgThreads);
+        cfg.dynamicSmemBytes   = smem;
+        cfg.attrs              = at;
+        cfg.numAttrs           = 1;
+        int nclusters          = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_pcg_kernel, &cfg) == cudaSuccess && nclusters > 0)
+            size = kPcgMaxCta;
+    }
+    cudaGetLastError();
+    return size;
+}
+}  // namespace
+
+int coarse_pcg_cluster_size() { return pcg_cluster_size(0); }
+
+int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
+{
+    constexpr size_t kSmemLimit = 200 * 1024;
+    CoarsePcgArgs    args       = args_in;
+    const int        nc         = 10 * (args.nl - 1) * (args.nl - 1) * (args.nr - 1);
+    // cluster size first from the node table alone, then decide on matrix residency
+    int       cs  = 8;
+    int       cpc = (nc + kPcgMaxCta - 1) / kPcgMaxCta;
+    size_t    node_bytes = (static_cast<size_t>(48) * cpc + 15) / 16 * 16;
+    size_t    smem       = node_bytes + static_cast<size_t>(342 * 8) * cpc;
+    bool      in_smem    = smem <= kSmemLimit;
+    if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(in_smem ? smem : node_bytes)) != cudaSuccess) {
+        cudaGetLastError();
+        return -2;
+    }
+    cs = pcg_cluster_size(in_smem ? smem : node_bytes);
+    if (cs != kPcgMaxCta) {
+        cpc        = (nc + cs - 1) / cs;
+        node_bytes = (static_cast<size_t>(48) * cpc + 15) / 16 * 16;
+        smem       = node_bytes + static_cast<size_t>(342 * 8) * cpc;
+        in_smem    = smem <= kSmemLimit;
+        if (!in_smem) smem = node_bytes;
+        if (node_bytes > kSmemLimit) return -1;
+        if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)) != cudaSuccess) {
+            cudaGetLastError();
+            return -2;
+        }
+    } else if (!in_smem) {
+        smem = node_bytes;
+        if (node_bytes > kSmemLimit) return -1;
+    }
+    args.cells_per_cta = cpc;
+    args.node_bytes    = static_cast<int>(node_bytes);
+    args.mats_in_smem  = in_smem ? 1 : 0;
+    cudaLaunchConfig_t  cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id               = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim            = dim3(cs);
+    cfg.blockDim           = dim3(kPcgThreads);
+    cfg.dynamicSmemBytes   = smem;
+    cfg.stream             = st;
+    cfg.attrs              = at;
+    cfg.numAttrs           = 1;
+    if (cudaLaunchKernelEx(&cfg, coarse_pcg_kernel, args) != cudaSuccess) {
+        cudaGetLastError();
+        return -2;
+    }
+    return 0;
+}
+
+int coarse_pcg_partials_size() { return 2 * kPcgMaxCta; }
+
+int coefficient_inject(int nlc, int nrc, const double* fine, double* coarse, bool reciprocal, cudaStream_t st)
+{
+    inject_kernel<<<grid_for(10ll * nlc * nlc * nrc), kThreads, 0, st>>>(nlc, nrc, fine, coarse, reciprocal ? 1 : 0);
+    return launch_status();
+}
+
+int cell_coefficient_average(int nlc, int nrc, const double* fine, double* coarse, cudaStream_t st)
+{
+    cell_average_kernel<<<grid_for(10ll * nlc * nlc * nrc), kThreads, 0, st>>>(nlc, nrc, fine, coarse);
+    return launch_status();
+}
+
+}  // namespace tn

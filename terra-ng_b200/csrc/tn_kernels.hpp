@@ -103,4 +103,111 @@ int max_abs_and_nan(int64_t n, int ncomp, const T* const* a, double* out_dev, in
 int convert_f64_to_f32(int64_t n, const double* in, float* out, cudaStream_t stream);
 int convert_f32_to_f64(int64_t n, const float* in, double* out, cudaStream_t stream);
 
+// ----------------------------------------------------------------------------
+// Galerkin coarse operators and stored element matrices (gca.cu). Matrices
+// are packed symmetric, 171 values per wedge, value-major: [w * 171 + p][cell].
+// ----------------------------------------------------------------------------
+int gca_values_per_cell();
+// coarse = sum P^T A_f P (fine level nlf, nrf); A_f from the nodal / cell
+// coefficient (on-the-fly element matrices) or from stored fine matrices.
+int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
+              const double* fine_mats, double* coarse_mats, cudaStream_t st);
+// element matrices of a level (the stored form of the on-the-fly operator)
+int element_matrices(int nl, int nr, const double* coords, const double* radii, const double* k, const double* kq0,
+                     double* mats, cudaStream_t st);
+// bake Dirichlet masks / free-slip rotations of the boundary cells into mats
+int gca_bake_boundary(int nl, int nr, const double* coords, const double* radii, int bc_cmb, int bc_surf, double* mats,
+                      cudaStream_t st);
+// dst += A src with baked matrices
+template <typename T>
+int gca_apply_add(int nl, int nr, const T* mats, const T* const* src, T* const* dst, cudaStream_t st);
+// dst += diag-mode(A) src with unbaked matrices
+int gca_diag_add(int nl, int nr, const double* coords, const double* radii, int bc_cmb, int bc_surf,
+                 const double* mats, const double* const* src, double* const* dst, cudaStream_t st);
+int gca_to_f32(int64_t n, const double* in, float* out, cudaStream_t st);
+
+// ----------------------------------------------------------------------------
+// Solver kernels (solver_kernels.cu).
+// A (block) vector is one allocation holding segments of components: a
+// component of segment s starts at seg[s].offset + c * seg[s].stride and has
+// seg[s].n valid entries; owned flags are per lateral node (entry / nr).
+// ----------------------------------------------------------------------------
+struct VecSeg {
+    int64_t        offset = 0, n = 0, stride = 0;
+    int            ncomp = 0, nr = 1;
+    const uint8_t* owned = nullptr;
+};
+struct VecDesc {
+    int     nseg = 0;
+    VecSeg  seg[2];
+    int64_t total = 0;  // allocation length in elements (padding included)
+};
+// Per-block partials (solver_partials_size() doubles) and a zero-initialised
+// completion counter that the last block resets.
+struct RedScratch {
+    double*   partials = nullptr;
+    unsigned* counter  = nullptr;
+};
+constexpr int kMaxAxpy = 64;
+struct AxpyList {
+    const double* z[kMaxAxpy];
+    double        y[kMaxAxpy];
+    int           m = 0;
+};
+struct CoarsePcgArgs {
+    int            nl = 0, nr = 0;
+    const double*  mats        = nullptr;  // baked stored matrices of the level
+    int            num_classes = 0;
+    const int32_t* off = nullptr;
+    const int32_t* mem = nullptr;
+    const uint8_t* owned = nullptr;
+    int64_t        n = 0, stride = 0;  // entries per component, component stride
+    double*        x  = nullptr;       // in: initial guess, out: solution
+    const double*  b  = nullptr;
+    double*        r  = nullptr;
+    double*        p  = nullptr;
+    double*        ap = nullptr;
+    double*        partials = nullptr;  // coarse_pcg_partials_size() doubles
+    int            max_iter = 50;
+    double         rtol = 1e-6, atol = 1e-16;
+    double*        stats = nullptr;  // [iterations, initial residual, final residual] or nullptr
+    // set by coarse_pcg: cells per CTA, bytes of the node table, matrices in shared memory
+    int cells_per_cta = 0, node_bytes = 0, mats_in_smem = 0;
+};
+int solver_partials_size();
+template <typename T>
+int vec_dot(const VecDesc& L, const T* a, const T* b, double* out_dev, RedScratch rs, bool take_sqrt, cudaStream_t st);
+// w -= (*h_sub) v_sub (when v_sub), then *out = <w, v_dot> or ||w|| (v_dot == nullptr)
+int mgs_step(const VecDesc& L, double* w, const double* v_sub, const double* h_sub, const double* v_dot, double* out,
+             RedScratch rs, cudaStream_t st);
+// x += a p, r -= a ap with a = *s_an / *s_ad; *out = ||r|| (or -1 when
+// |*s_ad| < DBL_MIN, in which case nothing is updated)
+int cg_update(const VecDesc& L, double* x, double* r, const double* p, const double* ap, const double* s_an,
+              const double* s_ad, double* out, RedScratch rs, cudaStream_t st);
+// p = z + (*s_num / *s_den) p (flat)
+int p_update(int64_t n, double* p, const double* z, const double* s_num, const double* s_den, cudaStream_t st);
+// y = x / *s_dev (flat over n entries)
+template <typename T>
+int scale_by_recip(int64_t n, T* y, const T* x, const double* s_dev, cudaStream_t st);
+// Chebyshev step: d = alpha D^-1 (b - ax) [+ beta d], x += d (flat)
+template <typename T>
+int cheb_step(int64_t n, T* x, T* d, const T* b, const T* ax, const T* invdiag, T alpha, T beta, bool first,
+              cudaStream_t st);
+// y = c (a .* b) (flat)
+template <typename T>
+int vec_mul(int64_t n, T* y, const T* a, const T* b, T c, cudaStream_t st);
+// x += sum_k y_k z_k (flat)
+int multi_axpy(int64_t n, double* x, const AxpyList& list, cudaStream_t st);
+// v = uniform(-1, 1) from SplitMix64 of (seed, canonical node id, component):
+// duplicates of a node get the same value.
+template <typename T>
+int random_fill(int64_t n, int ncomp, T* const* comps, int nr, const int32_t* canon_lat, uint64_t seed,
+                cudaStream_t st);
+template <typename T>
+int flag_nonfinite(int64_t n, const T* a, int* flag_dev, cudaStream_t st);
+int widen_check(int64_t n, const float* in, double* out, int* flag_dev, cudaStream_t st);
+int coarse_pcg(const CoarsePcgArgs& args, cudaStream_t st);
+int coarse_pcg_partials_size();
+int coarse_pcg_cluster_size();
+
 }  // namespace tn

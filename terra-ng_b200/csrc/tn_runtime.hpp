@@ -108,6 +108,7 @@ struct DeviceLevel {
     DevBuf     radii64, radii32;    // (nr)
     DevBuf     owned_lat;           // (10, nl, nl) uint8
     DevBuf     dup_offset, dup_members;
+    DevBuf     canon_lat;  // (10, nl, nl) int32: lowest lateral index of the node's duplicate class
     IfaceTable iface;
 
     int     nl() const { return host.nl; }
@@ -176,18 +177,35 @@ struct Operator {
     const DeviceLevel& lvl() const { return shell->level(level); }
 };
 
-// epsilon-div-div (EpsilonDivDivKerngen).
+// epsilon-div-div (EpsilonDivDivKerngen). With stored matrices (GCA levels,
+// OperatorStoredMatrixMode::Full) the apply runs over the packed element
+// matrices instead of the coefficient; boundary conditions are baked into a
+// copy of the matrices the first time an apply needs them.
 struct EpsDivDivOp : Operator {
-    DevBuf k;  // nodal or cell coefficient in `precision`
+    DevBuf k;  // nodal or cell coefficient in `precision` (may be empty in stored mode)
     bool   q0 = false;
     bool   diagonal = false;
     int    tile_y = 0, chunk_x = 0;
-    int    src_components() const override { return 3; }
-    int    dst_components() const override { return 3; }
-    void   apply(void* const* src, void* const* dst, cudaStream_t st) override;
+
+    bool   stored = false;
+    DevBuf mats;              // FP64 unbaked element matrices [342][cells]
+    DevBuf baked64, baked32;  // boundary-baked copies (built lazily)
+    int    baked_bc[2]   = {-1, -1};
+    bool   baked32_valid = false;
+
+    int  src_components() const override { return 3; }
+    int  dst_components() const override { return 3; }
+    void apply(void* const* src, void* const* dst, cudaStream_t st) override;
     template <typename T>
-    void apply_t(const T* const* src, T* const* dst, cudaStream_t st) const;
+    void apply_t(const T* const* src, T* const* dst, cudaStream_t st);
+    // stored-matrix helpers
+    void ensure_baked(bool need32, cudaStream_t st);
+    void set_stored_matrices_from_coefficient(cudaStream_t st);  // element matrices of this level
+    int64_t mats_values() const;
 };
+// TwoGridGCA (gca.hpp:41-531): coarse.mats = sum P^T A_fine P with A_fine the
+// fine operator's stored matrices or its on-the-fly Neumann element matrices.
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st);
 
 // B (DivergenceKerngen): velocity level -> pressure level (level - 1).
 struct DivergenceOp : Operator {

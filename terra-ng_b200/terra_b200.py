@@ -24,6 +24,29 @@ REPLACE, ADD = 0, 1
 SKIP_COMMUNICATION, COMMUNICATE_ADDITIVELY = 0, 1
 
 _lib = None
+STORED_OFF, STORED_FULL = 0, 1
+
+
+class SolverOptions(ctypes.Structure):
+    """tn_solver_options."""
+
+    _fields_ = [
+        ("restart", ctypes.c_int),
+        ("max_iterations", ctypes.c_int),
+        ("relative_tolerance", ctypes.c_double),
+        ("absolute_tolerance", ctypes.c_double),
+        ("chebyshev_order", ctypes.c_int),
+        ("chebyshev_iterations", ctypes.c_int),
+        ("power_iterations", ctypes.c_int),
+        ("num_vcycles", ctypes.c_int),
+        ("coarse_max_iterations", ctypes.c_int),
+        ("coarse_relative_tolerance", ctypes.c_double),
+        ("coarse_absolute_tolerance", ctypes.c_double),
+        ("gca", ctypes.c_int),
+        ("mixed_precision", ctypes.c_int),
+        ("seed", ctypes.c_uint64),
+        ("normalize_pressure", ctypes.c_int),
+    ]
 
 
 class TerraError(RuntimeError):
@@ -75,6 +98,25 @@ def load(path: str = LIB_PATH):
         "tn_interface_sum": ([vp, i, i, i, vpp, vp], i),
         "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
         "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
+        "tn_vec_random": ([vp, i, i, i, ctypes.c_uint64, vpp, vp], i),
+        "tn_operator_set_stored_matrix_mode": ([vp, i, vp], i),
+        "tn_gca_build": ([vp, vp, vp], i),
+        "tn_operator_copy_local_matrices": ([vp, vp], i),
+        "tn_solver_options_default": ([ctypes.POINTER(SolverOptions)], None),
+        "tn_stokes_solver_create": ([vp, i, vp, vp, vp, i, i, ctypes.POINTER(SolverOptions), vp,
+                                     ctypes.POINTER(vp)], i),
+        "tn_velocity_solver_create": ([vp, i, vp, vp, i, i, ctypes.POINTER(SolverOptions), vp, ctypes.POINTER(vp)],
+                                      i),
+        "tn_solver_destroy": ([vp], None),
+        "tn_solver_solve": ([vp, vpp, vpp, vp], i),
+        "tn_solver_result": ([vp, ctypes.POINTER(i), dp, ctypes.POINTER(i)], i),
+        "tn_solver_history": ([vp, dp, i, ctypes.POINTER(i)], i),
+        "tn_solver_precondition": ([vp, vpp, vpp, vp], i),
+        "tn_solver_vcycle": ([vp, i, vpp, vpp, vp], i),
+        "tn_solver_level_lambda": ([vp, i, dp], i),
+        "tn_solver_inverse_diagonal": ([vp, i, vpp, vp], i),
+        "tn_solver_coarse_stats": ([vp, dp], i),
+        "tn_solver_level_matrices": ([vp, i, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -294,6 +336,36 @@ class EpsDivDiv(Operator):
     def set_tile(self, tile_y=0, chunk_x=0):
         _check(load().tn_operator_set_tile(self._h, tile_y, chunk_x))
 
+    def set_stored_matrix_mode(self, mode=STORED_FULL, stream=None):
+        _check(load().tn_operator_set_stored_matrix_mode(self._h, mode, _stream(stream)))
+
+    def local_matrices(self):
+        """(10, nl-1, nl-1, nr-1, 2, 18, 18) stored matrices (host)."""
+        import numpy as np
+
+        nl, nr = self.shell.dims(self.level)
+        out = np.zeros((10, nl - 1, nl - 1, nr - 1, 2, 18, 18))
+        _check(load().tn_operator_copy_local_matrices(self._h, out.ctypes.data))
+        return out
+
+
+def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None):
+    """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build)."""
+    _check(load().tn_gca_build(fine._h, coarse._h, _stream(stream)))
+
+
+def random_vector(shell: Shell, level: int, ncomp: int, seed: int, dtype=None, stream=None):
+    """tn_vec_random into new tensors of shape (ncomp, 10, nl, nl, nr)."""
+    import torch
+
+    dtype = dtype or torch.float64
+    nl, nr = shell.dims(level)
+    v = torch.empty((ncomp, 10, nl, nl, nr), dtype=dtype, device="cuda")
+    comps = [v[c] for c in range(ncomp)]
+    _check(load().tn_vec_random(shell.handle, level % shell.num_levels, _prec(dtype), ncomp, ctypes.c_uint64(seed),
+                                _ptrs(comps), _stream(stream)))
+    return v
+
 
 class Divergence(Operator):
     """B: velocity on `level` -> pressure on `level - 1` (tn_divergence_create)."""
@@ -363,3 +435,111 @@ def restrict(shell: Shell, fine_level: int, fine, coarse, stream=None):
     _check(load().tn_restrict(shell.handle, fine_level % shell.num_levels, _prec(cf[0].dtype), len(cf), _ptrs(cf),
                               _ptrs(cc), _stream(stream)))
     return coarse
+
+
+def solver_options(**kw) -> SolverOptions:
+    o = SolverOptions()
+    load().tn_solver_options_default(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class _Solver:
+    _h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tn_solver_destroy(self._h)
+            self._h = None
+
+    def solve(self, x, b, stream=None):
+        """x (initial guess, overwritten), b: component lists. Returns True when converged."""
+        cx, cb = _comps(x), _comps(b)
+        rc = load().tn_solver_solve(self._h, _ptrs(cx), _ptrs(cb), _stream(stream))
+        if rc == -7:
+            return False
+        _check(rc)
+        return True
+
+    def result(self):
+        it, rr, cv = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _check(load().tn_solver_result(self._h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(cv)))
+        return it.value, rr.value, bool(cv.value)
+
+    def history(self):
+        n = ctypes.c_int()
+        _check(load().tn_solver_history(self._h, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_double * max(n.value, 1))()
+        _check(load().tn_solver_history(self._h, buf, n.value, ctypes.byref(n)))
+        return list(buf[: n.value])
+
+    def precondition(self, v, z, stream=None):
+        _check(load().tn_solver_precondition(self._h, _ptrs(_comps(v)), _ptrs(_comps(z)), _stream(stream)))
+        return z
+
+    def vcycle(self, x, b, stream=None):
+        cx, cb = _comps(x), _comps(b)
+        _check(load().tn_solver_vcycle(self._h, _prec(cx[0].dtype), _ptrs(cx), _ptrs(cb), _stream(stream)))
+        return x
+
+    def level_lambda(self, level):
+        out = ctypes.c_double()
+        _check(load().tn_solver_level_lambda(self._h, level, ctypes.byref(out)))
+        return out.value
+
+    def inverse_diagonal(self, level):
+        import torch
+
+        nl, nr = self.shell.dims(level)
+        out = torch.zeros((3, 10, nl, nl, nr), dtype=torch.float64, device="cuda")
+        _check(load().tn_solver_inverse_diagonal(self._h, level, _ptrs([out[c] for c in range(3)]), _stream(None)))
+        return out
+
+    def coarse_stats(self):
+        out = (ctypes.c_double * 3)()
+        _check(load().tn_solver_coarse_stats(self._h, out))
+        return list(out)
+
+    def level_matrices(self, level):
+        import numpy as np
+
+        nl, nr = self.shell.dims(level)
+        out = np.zeros((10, nl - 1, nl - 1, nr - 1, 2, 18, 18))
+        _check(load().tn_solver_level_matrices(self._h, level, out.ctypes.data))
+        return out
+
+
+def _opt_ptr(eta):
+    return None if eta is None else ctypes.c_void_p(eta.data_ptr())
+
+
+class StokesSolver(_Solver):
+    """FGMRES + block-triangular GMG preconditioner (tn_stokes_solver_create).
+    Vectors are 4 components (u_x, u_y, u_z on `level`, p on `level - 1`)."""
+
+    def __init__(self, shell: Shell, level: int = -1, eta=None, eta_cell=None, k_schur=None, bc_cmb=DIRICHLET,
+                 bc_surface=FREESLIP, stream=None, **options):
+        self.shell, self.level = shell, level % shell.num_levels
+        self.options = solver_options(**options)
+        h = ctypes.c_void_p()
+        _check(load().tn_stokes_solver_create(shell.handle, self.level, _opt_ptr(eta), _opt_ptr(eta_cell),
+                                              _opt_ptr(k_schur), bc_cmb, bc_surface, ctypes.byref(self.options),
+                                              _stream(stream), ctypes.byref(h)))
+        self._h = h
+
+
+class VelocitySolver(_Solver):
+    """CG on the epsilon-div-div operator with the GMG preconditioner (tn_velocity_solver_create)."""
+
+    def __init__(self, shell: Shell, level: int = -1, eta=None, eta_cell=None, bc_cmb=DIRICHLET,
+                 bc_surface=DIRICHLET, stream=None, **options):
+        self.shell, self.level = shell, level % shell.num_levels
+        self.options = solver_options(**options)
+        h = ctypes.c_void_p()
+        _check(load().tn_velocity_solver_create(shell.handle, self.level, _opt_ptr(eta), _opt_ptr(eta_cell), bc_cmb,
+                                                bc_surface, ctypes.byref(self.options), _stream(stream),
+                                                ctypes.byref(h)))
+        self._h = h

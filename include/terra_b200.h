@@ -59,6 +59,9 @@ typedef struct tn_solver   tn_solver;
 const char* tn_last_error(void);
 /* Library version string. */
 const char* tn_version(void);
+/* Kernel launches issued by this library since it was loaded (launch calls on
+ * any stream; for counting the device work of a call). */
+uint64_t tn_kernel_launch_count(void);
 
 /* ---- mesh hierarchy --------------------------------------------------------
  * Replaces DistributedDomain / DomainInfo with one subdomain per diamond plus
@@ -211,6 +214,8 @@ typedef struct tn_solver_options {
     uint64_t seed;                      /* power-iteration start vectors (12345) */
     int      normalize_pressure;        /* Stokes: subtract the owned-node pressure mean after the solve, as
                                            StokesContext::solve does (stokes_solver.hpp:684-690) (1) */
+    int      project_pressure_mean;     /* Stokes: iterate on P K, P removing the pressure mean, i.e. treat
+                                           constant pressure as a null vector; not in the reference (0) */
 } tn_solver_options;
 void tn_solver_options_default(tn_solver_options* opts);
 /* Stokes solve on velocity_level / velocity_level-1 (StokesContext,
@@ -239,6 +244,9 @@ int tn_solver_solve(tn_solver* solver, double* const* x_dev, const double* const
 /* Iterations (preconditioner applications), final relative residual
  * ||b - A x|| / ||b - A x0|| and whether the tolerance was met. */
 int tn_solver_result(const tn_solver* solver, int* iterations, double* relative_residual, int* converged);
+/* Stokes: final ||b - K x|| / ||b - K x0|| without the pressure-mean
+ * projection (equal to the relative residual when the projection is off). */
+int tn_solver_full_residual(const tn_solver* solver, double* relative_residual);
 /* Relative residual per iteration (history[0] = 1); *length = entries available. */
 int tn_solver_history(const tn_solver* solver, double* history_host, int capacity, int* length);
 /* z = M^-1 v: the block preconditioner (Stokes, 4 components) or the

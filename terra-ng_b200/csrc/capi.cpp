@@ -147,6 +147,8 @@ extern "C" {
 const char* tn_last_error(void) { return g_last_error.c_str(); }
 const char* tn_version(void) { return "terra_b200 0.1 (sm_100a)"; }
 
+uint64_t tn_kernel_launch_count(void) { return tn::launch_count(); }
+
 int tn_shell_create(int lat_level, int rad_level, int num_levels, double r_min, double r_max, tn_shell** out)
 {
     return guarded([&] {
@@ -636,6 +638,7 @@ void tn_solver_options_default(tn_solver_options* o)
     o->mixed_precision           = 0;
     o->seed                      = 12345;
     o->normalize_pressure        = 1;
+    o->project_pressure_mean     = 0;
 }
 
 int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,
@@ -654,7 +657,8 @@ int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* e
         so.rtol     = o.relative_tolerance;
         so.atol     = o.absolute_tolerance;
         so.mg       = mg_options(o);
-        so.normalize_pressure = o.normalize_pressure != 0;
+        so.normalize_pressure    = o.normalize_pressure != 0;
+        so.project_pressure_mean = o.project_pressure_mean != 0;
         auto s      = std::make_unique<tn_solver>();
         s->shell    = shell;
         s->stokes   = std::make_unique<tn::StokesSolver>(shell->impl.get(), velocity_level, eta_nodal_dev,
@@ -720,6 +724,14 @@ int tn_solver_result(const tn_solver* s, int* iterations, double* relative_resid
         if (iterations) *iterations = it;
         if (relative_residual) *relative_residual = rr;
         if (converged) *converged = cv ? 1 : 0;
+    });
+}
+
+int tn_solver_full_residual(const tn_solver* s, double* relative_residual)
+{
+    return guarded([&] {
+        need(s && relative_residual, "NULL argument");
+        *relative_residual = s->stokes ? s->stokes->full_relres : s->velocity->final_relres;
     });
 }
 

@@ -423,6 +423,7 @@ int launch_cfg(EddArgs<T> a, int nfields, cudaStream_t st)
     dim3      grid((nl + a.ty - 1) / a.ty, (nl + a.cx - 1) / a.cx, 10);
     dim3      block(32, a.ty + 1);
     k<<<grid, block, L.total, st>>>(a);
+    note_launch();
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

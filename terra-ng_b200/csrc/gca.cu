@@ -489,7 +489,11 @@ __global__ void f64_to_f32(int64_t n, const double* in, float* out)
         out[i] = static_cast<float>(in[i]);
 }
 
-inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+inline int launch_status(int kernels = 1)
+{
+    note_launch(kernels);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 inline dim3 cell_grid(int nl, int nr, int thr) { return dim3((nr - 1 + thr - 1) / thr, (nl - 1) * (nl - 1), 10); }
 
 }  // namespace

@@ -1,5 +1,6 @@
 // Host runtime: device mesh construction and operator dispatch.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include <type_traits>
@@ -7,6 +8,12 @@
 #include "tn_runtime.hpp"
 
 namespace tn {
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void     note_launch(int kernels) { g_launches.fetch_add(static_cast<uint64_t>(kernels), std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 int reduction_partials_size();
 

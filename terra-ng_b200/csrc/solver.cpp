@@ -608,6 +608,16 @@ void StokesSolver::copy_out(const DVec<double>& v, double* const* u, double* p, 
                "copy out");
 }
 
+// v_p -= (sum of v_p over owned pressure nodes) / (number of owned pressure nodes)
+void StokesSolver::remove_pressure_mean(DVec<double>& v, int slot, cudaStream_t st)
+{
+    const VecSeg& sp = blk_.seg[1];
+    const VecDesc pd = scalar_desc(sh_->level(vlevel_ - 1));
+    chk(vec_dot<double>(pd, v.data() + sp.offset, ones_p_.data(), scratch_.s(slot), scratch_.rs(), false, st), "sum");
+    chk(sub_scalar(sp.n, v.data() + sp.offset, scratch_.s(slot), 1.0 / static_cast<double>(num_owned_p_), st),
+        "shift");
+}
+
 void StokesSolver::precondition_external(const double* const* v, double* const* z, cudaStream_t st)
 {
     copy_in(r_, v, v[3], st);
@@ -631,17 +641,29 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
     copy_in(x_, u, p, st);
     copy_in(b_, fu, fp, st);
 
+    // With project_pressure_mean the iteration runs on P K with P removing the
+    // pressure mean (constant pressure treated as a null vector): with a
+    // free-slip surface the divergence rows keep a uniform part
+    // 1^T B u = (B^T 1)^T u != 0 (nodal normals are not the facet normals) that
+    // the preconditioned system cannot reduce, so the unprojected residual
+    // floors at an O(h^2) level. full_relres reports the unprojected residual.
     const double one_m[2] = {1.0, -1.0};
-    auto residual = [&]() {  // r = b - K x, returns ||r||
+    const int    kFull    = Scratch::kScalars - 2;  // scalar slots away from the Hessenberg column
+    auto residual = [&](bool report_full) {  // r = b - K x, returns ||r|| (projected when enabled)
         stokes_apply(x_, r_, st);
         lin<double>(nt, r_.data(), 0.0, 2, one_m, b_.data(), r_.data(), st);
+        if (report_full)
+            chk(vec_dot<double>(blk_, r_.data(), r_.data(), scratch_.s(kFull), scratch_.rs(), true, st), "norm");
+        if (opt_.project_pressure_mean) remove_pressure_mean(r_, kFull + 1, st);
         chk(vec_dot<double>(blk_, r_.data(), r_.data(), scratch_.s(0), scratch_.rs(), true, st), "norm");
-        scratch_.fetch(1, st);
+        scratch_.fetch(Scratch::kScalars, st);
         return scratch_.host[0];
     };
-    double       beta0 = residual();
+    double       beta0 = residual(true);
+    const double init_full = scratch_.host[kFull];
     const double init  = beta0;
     history.push_back(1.0);
+    full_relres = 1.0;
     if (beta0 <= opt_.atol || !(init > 0.0)) {
         converged = true;
         copy_out(x_, u, p, st);
@@ -667,6 +689,7 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
             precondition(V_[j], Zj, st);
             for (int attempt = 0; attempt < 2; ++attempt) {
                 stokes_apply(Zj, w_, st);
+                if (opt_.project_pressure_mean) remove_pressure_mean(w_, kFull + 1, st);
                 for (int i = 0; i <= j; ++i)
                     chk(mgs_step(blk_, w_.data(), i > 0 ? V_[i - 1].data() : nullptr, scratch_.s(H0 + i - 1),
                                  V_[i].data(), scratch_.s(H0 + i), scratch_.rs(), st),
@@ -732,8 +755,9 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
             }
             chk(multi_axpy(nt, x_.data(), L, st), "update");
         }
-        beta0        = residual();
+        beta0        = residual(true);
         final_relres = beta0 / init;
+        full_relres  = init_full > 0.0 ? scratch_.host[kFull] / init_full : 0.0;
         if (!std::isfinite(beta0)) break;
         if (beta0 <= opt_.atol || beta0 / init <= opt_.rtol) {
             converged = true;

@@ -152,6 +152,14 @@ __global__ void p_update_kernel(int64_t n, double* __restrict__ p, const double*
         p[i] = z[i] + beta * p[i];
 }
 
+// v -= scale * (*s) on n entries
+__global__ void sub_scalar_kernel(int64_t n, double* __restrict__ v, const double* s, double scale)
+{
+    const double  c      = scale * *s;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) v[i] -= c;
+}
+
 template <typename T>
 __global__ void scale_recip_kernel(int64_t n, T* __restrict__ y, const T* __restrict__ x, const double* s)
 {
@@ -516,7 +524,11 @@ inline int grid_for(int64_t n)
     if (b < 1) b = 1;
     return static_cast<int>(b);
 }
-inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+inline int launch_status(int kernels = 1)
+{
+    note_launch(kernels);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 }  // namespace
 
@@ -542,6 +554,12 @@ int cg_update(const VecDesc& L, double* x, double* r, const double* p, const dou
               const double* s_ad, double* out, RedScratch rs, cudaStream_t st)
 {
     cg_update_kernel<<<kBlocks, kThreads, 0, st>>>(L, x, r, p, ap, s_an, s_ad, rs, out);
+    return launch_status();
+}
+
+int sub_scalar(int64_t n, double* v, const double* s_dev, double scale, cudaStream_t st)
+{
+    sub_scalar_kernel<<<grid_for(n), kThreads, 0, st>>>(n, v, s_dev, scale);
     return launch_status();
 }
 
@@ -697,6 +715,7 @@ int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
     cfg.stream             = st;
     cfg.attrs              = at;
     cfg.numAttrs           = 1;
+    note_launch();
     if (cudaLaunchKernelEx(&cfg, coarse_pcg_kernel, args) != cudaSuccess) {
         cudaGetLastError();
         return -2;

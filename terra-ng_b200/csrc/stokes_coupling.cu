@@ -284,7 +284,11 @@ __global__ void vector_mass_kernel(int nl, int nr, const T* coords, const T* rad
     }
 }
 
-inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+inline int launch_status(int kernels = 1)
+{
+    note_launch(kernels);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 inline dim3 cell_grid(int nl, int nr, int threads) { return dim3((nr - 1 + threads - 1) / threads, (nl - 1) * (nl - 1), 10); }
 

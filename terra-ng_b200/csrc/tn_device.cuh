@@ -8,6 +8,7 @@
 
 namespace tn {
 
+
 // Device-side error codes written to the per-context error word.
 enum DeviceError : int {
     kDevOk             = 0,

@@ -8,6 +8,10 @@
 
 namespace tn {
 
+// Kernel launches issued by the library (counter in runtime.cpp).
+void     note_launch(int kernels = 1);
+uint64_t launch_count();
+
 // ----------------------------------------------------------------------------
 // epsilon-div-div apply (epsdivdiv.cu)
 // ----------------------------------------------------------------------------
@@ -184,6 +188,8 @@ int mgs_step(const VecDesc& L, double* w, const double* v_sub, const double* h_s
 // |*s_ad| < DBL_MIN, in which case nothing is updated)
 int cg_update(const VecDesc& L, double* x, double* r, const double* p, const double* ap, const double* s_an,
               const double* s_ad, double* out, RedScratch rs, cudaStream_t st);
+// v -= scale * *s_dev on n entries
+int sub_scalar(int64_t n, double* v, const double* s_dev, double scale, cudaStream_t st);
 // p = z + (*s_num / *s_den) p (flat)
 int p_update(int64_t n, double* p, const double* z, const double* s_num, const double* s_den, cudaStream_t st);
 // y = x / *s_dev (flat over n entries)

@@ -155,6 +155,7 @@ struct Shell {
     int* err_word() const { return err.as<int>(); }
 };
 
+
 std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, double r_min, double r_max);
 
 // Operator objects behind tn_operator. Vector arguments are arrays of

@@ -111,6 +111,7 @@ struct StokesOptions {
     int       restart = 30, max_iter = 300;
     double    rtol = 1e-8, atol = 1e-12;
     bool      normalize_pressure = true;
+    bool      project_pressure_mean = false;  // treat constant pressure as a null vector (see solve())
     MgOptions mg;
 };
 
@@ -134,6 +135,7 @@ class StokesSolver {
     std::vector<double> history;  // relative residual estimates, history[0] = 1
     int                 iterations = 0;
     double              final_relres = 0.0;
+    double              full_relres  = 0.0;  // ||b - K x|| / ||b - K x0|| without the pressure-mean projection
     bool                converged = false;
     VelocityMultigrid&  mg() { return *mg_; }
     const StokesOptions& options() const { return opt_; }
@@ -143,6 +145,7 @@ class StokesSolver {
     void stokes_apply(const DVec<double>& x, DVec<double>& y, cudaStream_t st);
     void copy_in(DVec<double>& v, const double* const* u, const double* p, cudaStream_t st);
     void copy_out(const DVec<double>& v, double* const* u, double* p, cudaStream_t st);
+    void remove_pressure_mean(DVec<double>& v, int slot, cudaStream_t st);
 
     const Shell*                       sh_;
     int                                vlevel_;

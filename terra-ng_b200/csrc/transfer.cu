@@ -102,7 +102,11 @@ __global__ void restrict_kernel(int nlf, int nrf, int ncomp, const uint8_t* __re
     for (int c = 0; c < ncomp; ++c) P.out[c][ci] = acc[c];
 }
 
-inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+inline int launch_status(int kernels = 1)
+{
+    note_launch(kernels);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 }  // namespace
 

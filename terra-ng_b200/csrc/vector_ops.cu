@@ -190,7 +190,11 @@ inline int grid_for(int64_t n, int threads)
     return static_cast<int>(b);
 }
 
-inline int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+inline int launch_status(int kernels = 1)
+{
+    note_launch(kernels);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 }  // namespace
 
@@ -267,7 +271,7 @@ int masked_dot(int64_t n, int nr, int ncomp, const uint8_t* owned_lat, const T* 
     }
     dot_partial_kernel<T><<<kRedBlocks, kRedThreads, 0, stream>>>(n, nr, ncomp, owned_lat, aa, bb, partials);
     finish_sum_kernel<<<1, 1024, 0, stream>>>(partials, kRedBlocks, out_dev);
-    return launch_status();
+    return launch_status(2);
 }
 
 template <typename T>
@@ -279,7 +283,7 @@ int max_abs_and_nan(int64_t n, int ncomp, const T* const* a, double* out_dev, in
     // partial maxima go to out_dev[1 .. kRedBlocks]
     maxabs_kernel<T><<<kRedBlocks, kRedThreads, 0, stream>>>(n, ncomp, aa, out_dev + 1, nan_dev);
     finish_max_kernel<<<1, 32, 0, stream>>>(out_dev + 1, kRedBlocks, out_dev);
-    return launch_status();
+    return launch_status(2);
 }
 
 int convert_f64_to_f32(int64_t n, const double* in, float* out, cudaStream_t stream)

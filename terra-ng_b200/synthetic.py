@@ -1,0 +1,123 @@
+"""Seeded synthetic inputs for the Stokes workloads (no datasets are involved).
+
+* viscosity: eta = exp(A * s(x_hat) * cos(pi (r - r_min) / (r_max - r_min))),
+  s = sum of 8 real spherical harmonics of degree <= 4 with seeded (l, m, c),
+  normalised to max |s| = 1 over the level's nodes; A = ln(10) gives a contrast
+  of 10^2 (eta in [0.1, 10]). Real harmonics are the orthonormal ones built
+  from the associated Legendre recursion (written here, not taken from the
+  reference's SphericalHarmonicsTool).
+* temperature: a smooth field of the same kind (8 harmonics times sin(pi
+  (r - r_min) / (r_max - r_min))) plus N(0, 0.01) noise drawn per unique node.
+* buoyancy right-hand side f = M (T r_hat) with the vector mass matrix, then
+  Dirichlet rows zeroed and free-slip normal components removed (the app's
+  RHS assembly, apps/mantlecirculation/src/stokes_solver.hpp:650-671).
+
+Every field is a function of the node's physical position (or of its
+canonical node id for the noise), so interface duplicates are equal.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+import terra_b200 as T
+
+
+def _assoc_legendre(lmax, x):
+    """P_l^m(x) for 0 <= m <= l <= lmax (Condon-Shortley phase omitted)."""
+    P = {}
+    s = np.sqrt(np.maximum(0.0, 1.0 - x * x))
+    P[(0, 0)] = np.ones_like(x)
+    for m in range(1, lmax + 1):
+        P[(m, m)] = (2 * m - 1) * s * P[(m - 1, m - 1)]
+    for m in range(0, lmax):
+        P[(m + 1, m)] = (2 * m + 1) * x * P[(m, m)]
+    for m in range(0, lmax + 1):
+        for l in range(m + 2, lmax + 1):
+            P[(l, m)] = ((2 * l - 1) * x * P[(l - 1, m)] - (l + m - 1) * P[(l - 2, m)]) / (l - m)
+    return P
+
+
+def real_sh(l, m, xyz):
+    """Orthonormal real spherical harmonic Y_lm at unit vectors xyz (..., 3)."""
+    x, y, z = xyz[..., 0], xyz[..., 1], xyz[..., 2]
+    phi = np.arctan2(y, x)
+    P = _assoc_legendre(l, np.clip(z, -1.0, 1.0))
+    am = abs(m)
+    norm = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - am) / math.factorial(l + am))
+    if m == 0:
+        return norm * P[(l, 0)]
+    if m > 0:
+        return math.sqrt(2.0) * norm * P[(l, am)] * np.cos(am * phi)
+    return math.sqrt(2.0) * norm * P[(l, am)] * np.sin(am * phi)
+
+
+def _harmonic_sum(xhat, seed, terms=8, lmax=4):
+    rng = np.random.default_rng(seed)
+    s = np.zeros(xhat.shape[:-1])
+    for _ in range(terms):
+        l = int(rng.integers(1, lmax + 1))
+        m = int(rng.integers(-l, l + 1))
+        c = rng.standard_normal()
+        s += c * real_sh(l, m, xhat)
+    return s / np.abs(s).max()
+
+
+def _geometry(shell: "T.Shell", level: int):
+    coords = shell.coords(level)  # (10, nl, nl, 3) unit vectors
+    radii = shell.radii(level)
+    return coords, radii
+
+
+def viscosity(shell: "T.Shell", level: int, seed: int = 1, log_amplitude: float = math.log(10.0)):
+    """Nodal viscosity (10, nl, nl, nr) as a numpy array."""
+    coords, radii = _geometry(shell, level)
+    s = _harmonic_sum(coords, seed)  # (10, nl, nl)
+    rad = np.cos(math.pi * (radii - radii[0]) / (radii[-1] - radii[0]))
+    return np.exp(log_amplitude * s[..., None] * rad[None, None, None, :])
+
+
+def temperature(shell: "T.Shell", level: int, seed: int = 2, noise: float = 0.01):
+    """Temperature (10, nl, nl, nr): smooth harmonics plus N(0, noise^2) per unique node (device tensor)."""
+    import torch
+
+    coords, radii = _geometry(shell, level)
+    s = _harmonic_sum(coords, seed)
+    rad = np.sin(math.pi * (radii - radii[0]) / (radii[-1] - radii[0]))
+    t = torch.tensor(s[..., None] * rad[None, None, None, :], device="cuda")
+    # Box-Muller on two seeded uniform fields that agree on interface duplicates
+    u = T.random_vector(shell, level, 2, seed * 1000003 + 17)
+    u1 = (0.5 * (u[0] + 1.0)).clamp_min(1e-300)
+    u2 = 0.5 * (u[1] + 1.0)
+    t += noise * torch.sqrt(-2.0 * torch.log(u1)) * torch.cos(2.0 * math.pi * u2)
+    return t
+
+
+def buoyancy_rhs(shell: "T.Shell", level: int, temp, bc_cmb: int, bc_surface: int):
+    """f = M (T r_hat) with boundary rows enforced; (3, 10, nl, nl, nr) device tensor."""
+    import torch
+
+    coords, radii = _geometry(shell, level)
+    n = torch.tensor(coords, device="cuda").permute(3, 0, 1, 2)  # (3, 10, nl, nl)
+    src = (temp[None] * n[..., None]).contiguous()
+    f = torch.zeros_like(src)
+    T.vector_mass_apply(shell, level, src, f)
+    return enforce_boundary(shell, level, f, bc_cmb, bc_surface)
+
+
+def enforce_boundary(shell: "T.Shell", level: int, f, bc_cmb: int, bc_surface: int):
+    """Zero Dirichlet rows and remove free-slip normal components
+    (strong_algebraic_dirichlet_enforcement.hpp:114-123,
+    strong_algebraic_freeslip_enforcement.hpp:22-38)."""
+    import torch
+
+    coords, _ = _geometry(shell, level)
+    n = torch.tensor(coords, device="cuda").permute(3, 0, 1, 2)
+    for side, bc in ((0, bc_cmb), (-1, bc_surface)):
+        if bc == T.DIRICHLET:
+            f[..., side] = 0.0
+        elif bc == T.FREESLIP:
+            dn = (f[..., side] * n).sum(0)
+            f[..., side] -= dn[None] * n
+    return f

@@ -46,6 +46,7 @@ class SolverOptions(ctypes.Structure):
         ("mixed_precision", ctypes.c_int),
         ("seed", ctypes.c_uint64),
         ("normalize_pressure", ctypes.c_int),
+        ("project_pressure_mean", ctypes.c_int),
     ]
 
 
@@ -69,6 +70,7 @@ def load(path: str = LIB_PATH):
     sig = {
         "tn_last_error": ([], ctypes.c_char_p),
         "tn_version": ([], ctypes.c_char_p),
+        "tn_kernel_launch_count": ([], ctypes.c_uint64),
         "tn_shell_create": ([i, i, i, d, d, ctypes.POINTER(vp)], i),
         "tn_shell_destroy": ([vp], None),
         "tn_shell_num_levels": ([vp, ctypes.POINTER(i)], i),
@@ -111,6 +113,7 @@ def load(path: str = LIB_PATH):
         "tn_solver_solve": ([vp, vpp, vpp, vp], i),
         "tn_solver_result": ([vp, ctypes.POINTER(i), dp, ctypes.POINTER(i)], i),
         "tn_solver_history": ([vp, dp, i, ctypes.POINTER(i)], i),
+        "tn_solver_full_residual": ([vp, dp], i),
         "tn_solver_precondition": ([vp, vpp, vpp, vp], i),
         "tn_solver_vcycle": ([vp, i, vpp, vpp, vp], i),
         "tn_solver_level_lambda": ([vp, i, dp], i),
@@ -124,6 +127,11 @@ def load(path: str = LIB_PATH):
         f.restype = res
     _lib = L
     return L
+
+
+def kernel_launch_count() -> int:
+    """Kernel launches issued by the library so far (tn_kernel_launch_count)."""
+    return int(load().tn_kernel_launch_count())
 
 
 def declared_symbols(header: str = HEADER_PATH):
@@ -468,6 +476,11 @@ class _Solver:
         it, rr, cv = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
         _check(load().tn_solver_result(self._h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(cv)))
         return it.value, rr.value, bool(cv.value)
+
+    def full_residual(self):
+        out = ctypes.c_double()
+        _check(load().tn_solver_full_residual(self._h, ctypes.byref(out)))
+        return out.value
 
     def history(self):
         n = ctypes.c_int()

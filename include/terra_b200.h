@@ -131,6 +131,16 @@ int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x);
  * (tn_operator_components). */
 int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* dst_dev, void* stream);
 
+/* Backward of tn_operator_apply for an epsilon-div-div operator with a
+ * per-cell (Q0) coefficient (no counterpart in the reference, which has no
+ * adjoint): grad_logeta_cell_dev[e] = d(lambda^T A u)/d log(eta_e) =
+ * lambda_e^T A_e(eta_e) u_e, boundary treatment included, written (not
+ * accumulated); when grad_u_dev is not NULL also grad_u = A^T lambda = A lambda
+ * (A is symmetric; the operator's communication mode applies). Arrays in the
+ * operator's precision; u and lambda are consistent (assembled) vectors. */
+int tn_epsdivdiv_vjp(tn_operator* op, const void* const* u_dev, const void* const* lambda_dev,
+                     void* grad_logeta_cell_dev, void* const* grad_u_dev, void* stream);
+
 /* Lumped k-weighted pressure mass diagonal, 6-point rule, interface-summed
  * (KMass with set_lumped_diagonal, src/terra/fe/wedge/operators/shell/
  * kmass.hpp:98-181; used with k = 1/eta as the Schur preconditioner,
@@ -261,6 +271,16 @@ int tn_solver_level_lambda(tn_solver* solver, int level, double* lambda_max);
 int tn_solver_inverse_diagonal(tn_solver* solver, int level, double* const* out_dev, void* stream);
 /* [iterations, initial residual, final residual] of the last coarsest CG. */
 int tn_solver_coarse_stats(tn_solver* solver, double* stats3);
+/* Adjoint gradient of J = 1/2 sum over owned velocity nodes |u - u_obs|^2
+ * with respect to the per-cell log-viscosity of a Stokes solver created with
+ * eta_cell_dev (no counterpart in the reference): x_dev is the forward
+ * solution (4 components), u_obs_dev 3 components. One adjoint solve
+ * K lambda = [u - u_obs; 0] (boundary rows enforced) with the solver's FGMRES,
+ * then grad = -lambda_u^T dA/dlog(eta) u (tn_epsdivdiv_vjp). lambda_dev (4
+ * components) receives the adjoint solution when not NULL. Synchronous;
+ * TN_ERR_NOT_CONVERGED when the adjoint solve stopped early. */
+int tn_stokes_misfit_gradient(tn_solver* solver, const double* const* x_dev, const double* const* u_obs_dev,
+                              double* grad_logeta_cell_dev, double* const* lambda_dev, void* stream);
 /* stored matrices of coarse level 0..fine-1 of the hierarchy, layout as
  * tn_operator_copy_local_matrices. */
 int tn_solver_level_matrices(tn_solver* solver, int level, double* mats_host);

@@ -213,7 +213,7 @@ class EpsDivDiv:
         ll = [np.ascontiguousarray(lam[i]) for i in range(3)]
         rc = lib().tno_epsdivdiv_vjp_logeta(ctypes.byref(s), _dpp(uu), _dpp(ll), _dp(g))
         if rc != 0:
-            raise ValueError("vjp not supported for this operator")
+            raise ValueError("vjp needs a per-cell (Q0) coefficient")
         return g
 
 

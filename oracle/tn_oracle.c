@@ -424,8 +424,8 @@ static void physical_coords(const tno_op* op, int d, int x, int y, int r, double
 
 /* Slow-path cell apply (epsilon_divdiv_kerngen.hpp:1013-1242) given the two
  * (unmasked) wedge matrices. Adds into dst. */
-static void slow_cell(const tno_op* op, int d, int x, int y, int r, double A[2][324], const double* const* src,
-                      double* const* dst)
+static void slow_cell_local(const tno_op* op, int d, int x, int y, int r, double A[2][324], const double* const* src,
+                            double outw[2][18])
 {
     const int nl = op->nl, nr = op->nr;
     int       at_cmb = (r == 0), at_surface = (r + 1 == nr - 1);
@@ -522,10 +522,22 @@ static void slow_cell(const tno_op* op, int d, int x, int y, int r, double A[2][
             for (int dim = 0; dim < 3; dim++)
                 for (int n = 0; n < 6; n++) out[n + dim * 6] = o2[n * 3 + dim];
         }
+        for (int i = 0; i < 18; i++) outw[w][i] = out[i];
+    }
+}
+
+/* Slow-path cell apply: adds the cell's outputs into dst. */
+static void slow_cell(const tno_op* op, int d, int x, int y, int r, double A[2][324], const double* const* src,
+                      double* const* dst)
+{
+    const int nl = op->nl, nr = op->nr;
+    double    outw[2][18];
+    slow_cell_local(op, d, x, y, r, A, src, outw);
+    for (int w = 0; w < 2; w++)
         for (int dim = 0; dim < 3; dim++)
             for (int n = 0; n < 6; n++)
-                dst[dim][IDX4(nl, nr, d, x + WOFF[w][n][0], y + WOFF[w][n][1], r + WOFF[w][n][2])] += out[dim * 6 + n];
-    }
+                dst[dim][IDX4(nl, nr, d, x + WOFF[w][n][0], y + WOFF[w][n][1], r + WOFF[w][n][2])] +=
+                    outw[w][dim * 6 + n];
 }
 
 /* Cell loops are split into two x-parity sweeps so that concurrent threads
@@ -1256,39 +1268,26 @@ int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coar
 int tno_epsdivdiv_vjp_logeta(const tno_op* op, const double* const* u, const double* const* lam, double* g)
 {
     if (!op->k_q0) return -1;
-    if (op->bc_cmb == 2 || op->bc_surface == 2) return -2;
     const int nl = op->nl, nr = op->nr;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int d = 0; d < 10; d++)
         for (int x = 0; x < nl - 1; x++)
             for (int y = 0; y < nl - 1; y++)
                 for (int r = 0; r < nr - 1; r++) {
-                    const int at_cmb = (r == 0), at_surface = (r + 1 == nr - 1);
-                    const int bcf    = at_cmb ? op->bc_cmb : (at_surface ? op->bc_surface : 0);
-                    double    acc    = 0.0;
-                    for (int w = 0; w < 2; w++) {
-                        double A[324], su[18], sl[18];
-                        local_matrix(op, d, x, y, r, w, A);
-                        for (int dd = 0; dd < 3; dd++)
-                            for (int n = 0; n < 6; n++) {
-                                long id = IDX4(nl, nr, d, x + WOFF[w][n][0], y + WOFF[w][n][1], r + WOFF[w][n][2]);
-                                su[dd * 6 + n] = u[dd][id];
-                                sl[dd * 6 + n] = lam[dd][id];
-                            }
-                        for (int di = 0; di < 3; di++)
-                            for (int dj = 0; dj < 3; dj++)
-                                for (int i = 0; i < 6; i++)
-                                    for (int j = 0; j < 6; j++) {
-                                        if (op->diagonal && !(di == dj && i == j)) continue;
-                                        if ((at_cmb || at_surface) && bcf == 1 &&
-                                            ((at_cmb && ((di == dj && i != j && (i < 3 || j < 3)) ||
-                                                         (di != dj && (i < 3 || j < 3)))) ||
-                                             (at_surface && ((di == dj && i != j && (i >= 3 || j >= 3)) ||
-                                                             (di != dj && (i >= 3 || j >= 3))))))
-                                            continue;
-                                        acc += sl[i + 6 * di] * A[(i + 6 * di) * 18 + j + 6 * dj] * su[j + 6 * dj];
-                                    }
-                    }
+                    /* A is linear in eta_cell: d(lambda^T A u)/d log eta_cell is the
+                     * cell's own contribution lambda_e^T A_e(eta_cell) u_e, boundary
+                     * treatment included (slow path). */
+                    double A[2][324], outw[2][18];
+                    local_matrix(op, d, x, y, r, 0, A[0]);
+                    local_matrix(op, d, x, y, r, 1, A[1]);
+                    slow_cell_local(op, d, x, y, r, A, u, outw);
+                    double acc = 0.0;
+                    for (int w = 0; w < 2; w++)
+                        for (int dim = 0; dim < 3; dim++)
+                            for (int n = 0; n < 6; n++)
+                                acc += lam[dim][IDX4(nl, nr, d, x + WOFF[w][n][0], y + WOFF[w][n][1],
+                                                     r + WOFF[w][n][2])] *
+                                       outw[w][dim * 6 + n];
                     g[IDX4(nl - 1, nr - 1, d, x, y, r)] += acc;
                 }
     return 0;

@@ -82,8 +82,8 @@ int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coar
 double tno_masked_dot(int lat_level, int nr, int ncomp, const double* const* a, const double* const* b);
 
 /* adjoint / VJP with respect to per-cell log-viscosity for the Q0 coefficient:
- * g_cell += lambda^T dA/dlog(eta_cell) u, with the operator boundary handling
- * (Dirichlet / Neumann only). */
+ * g_cell += lambda^T dA/dlog(eta_cell) u = lambda_e^T A_e(eta_cell) u_e, with
+ * the operator's slow-path boundary handling (Neumann, Dirichlet, free-slip). */
 int tno_epsdivdiv_vjp_logeta(const tno_op* op, const double* const* u, const double* const* lam, double* g_cell);
 
 int tno_set_threads(int n);

@@ -803,6 +803,52 @@ int tn_solver_coarse_stats(tn_solver* s, double* stats3)
     });
 }
 
+int tn_epsdivdiv_vjp(tn_operator* op, const void* const* u_dev, const void* const* lambda_dev,
+                     void* grad_logeta_cell_dev, void* const* grad_u_dev, void* stream)
+{
+    return guarded([&] {
+        need(op && u_dev && lambda_dev && grad_logeta_cell_dev, "NULL argument");
+        auto* e = as_edd(op);
+        if (e->precision == TN_F64)
+            e->vjp_logeta<double>(reinterpret_cast<const double* const*>(u_dev),
+                                  reinterpret_cast<const double* const*>(lambda_dev),
+                                  static_cast<double*>(grad_logeta_cell_dev), as_stream(stream));
+        else
+            e->vjp_logeta<float>(reinterpret_cast<const float* const*>(u_dev),
+                                 reinterpret_cast<const float* const*>(lambda_dev),
+                                 static_cast<float*>(grad_logeta_cell_dev), as_stream(stream));
+        if (grad_u_dev) {
+            // A^T lambda = A lambda, Replace
+            const int am = e->apply_mode;
+            e->apply_mode = 0;
+            try {
+                e->apply(const_cast<void* const*>(lambda_dev), grad_u_dev, as_stream(stream));
+            } catch (...) {
+                e->apply_mode = am;
+                throw;
+            }
+            e->apply_mode = am;
+        }
+    });
+}
+
+int tn_stokes_misfit_gradient(tn_solver* s, const double* const* x_dev, const double* const* u_obs_dev,
+                              double* grad_logeta_cell_dev, double* const* lambda_dev, void* stream)
+{
+    int       converged = 0;
+    const int rc        = guarded([&] {
+        need(s && x_dev && u_obs_dev && grad_logeta_cell_dev, "NULL argument");
+        need(s->stokes != nullptr, "not a Stokes solver");
+        converged = s->stokes->misfit_gradient(x_dev, u_obs_dev, grad_logeta_cell_dev, lambda_dev, as_stream(stream));
+    });
+    if (rc != TN_OK) return rc;
+    if (!converged) {
+        g_last_error = "the adjoint solve stopped before reaching its tolerance";
+        return TN_ERR_NOT_CONVERGED;
+    }
+    return TN_OK;
+}
+
 int tn_solver_level_matrices(tn_solver* s, int level, double* mats_host)
 {
     return guarded([&] {

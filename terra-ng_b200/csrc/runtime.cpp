@@ -148,6 +148,31 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st)
 }
 
 template <typename T>
+void EpsDivDivOp::vjp_logeta(const T* const* u, const T* const* lam, T* grad_cell, cudaStream_t st) const
+{
+    if (!q0 || k.get() == nullptr)
+        throw Error(kErrUnsupported, "the log-viscosity gradient needs a per-cell (Q0) coefficient");
+    if (stored) throw Error(kErrUnsupported, "the log-viscosity gradient needs the matrix-free operator");
+    const DeviceLevel& L = lvl();
+    VjpLaunch<T>       p;
+    p.nl      = L.nl();
+    p.nr      = L.nr();
+    p.coords  = L.coords<T>();
+    p.radii   = L.radii<T>();
+    p.kq0     = k.as<T>();
+    p.bc_cmb  = bc_cmb;
+    p.bc_surf = bc_surf;
+    p.grad    = grad_cell;
+    for (int c = 0; c < 3; ++c) {
+        p.u[c]   = u[c];
+        p.lam[c] = lam[c];
+    }
+    if (epsdivdiv_vjp_logeta<T>(p, st) != 0) throw Error(kErrCuda, "vjp launch failed");
+}
+template void EpsDivDivOp::vjp_logeta<double>(const double* const*, const double* const*, double*, cudaStream_t) const;
+template void EpsDivDivOp::vjp_logeta<float>(const float* const*, const float* const*, float*, cudaStream_t) const;
+
+template <typename T>
 void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
 {
     const DeviceLevel& L = lvl();

@@ -629,6 +629,58 @@ void StokesSolver::precondition_external(const double* const* v, double* const* 
 
 bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, const double* fp, cudaStream_t st)
 {
+    copy_in(x_, u, p, st);
+    copy_in(b_, fu, fp, st);
+    const bool ok = solve_internal(st);
+    copy_out(x_, u, p, st);
+    cuda_check(cudaStreamSynchronize(st), "synchronize");
+    return ok;
+}
+
+bool StokesSolver::misfit_gradient(const double* const* x, const double* const* u_obs, double* grad_cell,
+                                   double* const* lambda, cudaStream_t st)
+{
+    if (!K_.A.q0) throw Error(kErrUnsupported, "the log-viscosity gradient needs a per-cell viscosity");
+    const DeviceLevel& Lu = sh_->level(vlevel_);
+    const size_t       bu = sizeof(double) * Lu.nodes();
+    // adjoint right-hand side [u - u_obs; 0], boundary rows enforced
+    cuda_check(cudaMemsetAsync(b_.data(), 0, sizeof(double) * b_.total(), st), "zero");
+    for (int c = 0; c < 3; ++c) {
+        double*       y[1]  = {b_.comp(0, c)};
+        const double* x0[1] = {x[c]};
+        const double* x1[1] = {u_obs[c]};
+        const double  cf[2] = {1.0, -1.0};
+        chk(lincomb<double>(Lu.nodes(), 1, y, 0.0, 2, cf, x0, x1, nullptr, st), "misfit");
+    }
+    {
+        double* bc[3] = {b_.comp(0, 0), b_.comp(0, 1), b_.comp(0, 2)};
+        chk(enforce_velocity_bcs(Lu.nl(), Lu.nr(), Lu.coords<double>(), K_.A.bc_cmb, K_.A.bc_surf, bc, st), "bcs");
+    }
+    cuda_check(cudaMemsetAsync(x_.data(), 0, sizeof(double) * x_.total(), st), "zero");
+    const bool ok = solve_internal(st);
+    // grad = -lambda_u^T dA/dlog(eta) u
+    const double* uu[3] = {x[0], x[1], x[2]};
+    const double* ll[3] = {x_.comp(0, 0), x_.comp(0, 1), x_.comp(0, 2)};
+    K_.A.vjp_logeta<double>(uu, ll, grad_cell, st);
+    {
+        double*       g[1]  = {grad_cell};
+        const double* gi[1] = {grad_cell};
+        const double  neg   = -1.0;
+        chk(lincomb<double>(Lu.cells(), 1, g, 0.0, 1, &neg, gi, nullptr, nullptr, st), "negate");
+    }
+    if (lambda) {
+        for (int c = 0; c < 3; ++c)
+            cuda_check(cudaMemcpyAsync(lambda[c], x_.comp(0, c), bu, cudaMemcpyDeviceToDevice, st), "copy out");
+        cuda_check(cudaMemcpyAsync(lambda[3], x_.comp(1, 0), sizeof(double) * blk_.seg[1].n, cudaMemcpyDeviceToDevice,
+                                   st),
+                   "copy out");
+    }
+    cuda_check(cudaStreamSynchronize(st), "synchronize");
+    return ok;
+}
+
+bool StokesSolver::solve_internal(cudaStream_t st)
+{
     const double eps   = std::numeric_limits<double>::epsilon();
     const int    m     = opt_.restart;
     const int64_t nt   = blk_.total;
@@ -638,11 +690,9 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
     final_relres = 0.0;
     cuda_check(cudaMemsetAsync(scratch_.counter.get(), 0, sizeof(unsigned), st), "zero counter");
     cuda_check(cudaMemsetAsync(scratch_.flag_dev(), 0, sizeof(int), st), "zero flag");
-    copy_in(x_, u, p, st);
-    copy_in(b_, fu, fp, st);
 
-    // With project_pressure_mean the iteration runs on P K with P removing the
-    // pressure mean (constant pressure treated as a null vector): with a
+    // With project_pressure_mean the iteration runs on P K P with P removing
+    // the pressure mean (constant pressure treated as a null vector): with a
     // free-slip surface the divergence rows keep a uniform part
     // 1^T B u = (B^T 1)^T u != 0 (nodal normals are not the facet normals) that
     // the preconditioned system cannot reduce, so the unprojected residual
@@ -659,6 +709,10 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
         scratch_.fetch(Scratch::kScalars, st);
         return scratch_.host[0];
     };
+    // the iterate's pressure stays mean-free under the projection, so the
+    // iteration is on [A, B^T P; P B, 0] over mean-free pressures, which is
+    // symmetric and nonsingular (the solution is a function of the data)
+    if (opt_.project_pressure_mean) remove_pressure_mean(x_, kFull + 1, st);
     double       beta0 = residual(true);
     const double init_full = scratch_.host[kFull];
     const double init  = beta0;
@@ -666,8 +720,6 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
     full_relres = 1.0;
     if (beta0 <= opt_.atol || !(init > 0.0)) {
         converged = true;
-        copy_out(x_, u, p, st);
-        cuda_check(cudaStreamSynchronize(st), "synchronize");
         return true;
     }
     std::vector<double> H((m + 1) * m), g(m + 1), cs(m + 1), sn(m + 1), y(m);
@@ -687,6 +739,7 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
             ++steps;
             cuda_check(cudaMemsetAsync(Zj.data(), 0, sizeof(double) * nt, st), "zero");
             precondition(V_[j], Zj, st);
+            if (opt_.project_pressure_mean) remove_pressure_mean(Zj, kFull + 1, st);
             for (int attempt = 0; attempt < 2; ++attempt) {
                 stokes_apply(Zj, w_, st);
                 if (opt_.project_pressure_mean) remove_pressure_mean(w_, kFull + 1, st);
@@ -778,8 +831,6 @@ bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, c
         const double* src[1] = {x_.data() + sp.offset};
         chk(lincomb<double>(sp.n, 1, pc, -mean, 1, &one, src, nullptr, nullptr, st), "normalise");
     }
-    copy_out(x_, u, p, st);
-    cuda_check(cudaStreamSynchronize(st), "synchronize");
     return converged;
 }
 

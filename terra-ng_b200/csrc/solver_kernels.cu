@@ -517,6 +517,28 @@ __global__ void cell_average_kernel(int nlc, int nrc, const double* __restrict__
     }
 }
 
+// Strong boundary treatment of a velocity right-hand side: Dirichlet rows
+// zeroed, free-slip normal components removed (n = unit lateral coordinate).
+__global__ void enforce_bcs_kernel(int nl, int nr, const double* __restrict__ coords, int bc_cmb, int bc_surf,
+                                   CompPtrs<double> v)
+{
+    const int lat = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lat >= 10 * nl * nl) return;
+    const double* c = coords + static_cast<int64_t>(lat) * 3;
+    const double  m = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    const double  n[3] = {c[0] / m, c[1] / m, c[2] / m};
+    for (int side = 0; side < 2; ++side) {
+        const int     bc = side == 0 ? bc_cmb : bc_surf;
+        const int64_t id = static_cast<int64_t>(lat) * nr + (side == 0 ? 0 : nr - 1);
+        if (bc == 1) {
+            for (int k = 0; k < 3; ++k) v.p[k][id] = 0.0;
+        } else if (bc == 2) {
+            const double dn = n[0] * v.p[0][id] + n[1] * v.p[1][id] + n[2] * v.p[2][id];
+            for (int k = 0; k < 3; ++k) v.p[k][id] -= dn * n[k];
+        }
+    }
+}
+
 inline int grid_for(int64_t n)
 {
     int64_t b = (n + kThreads - 1) / kThreads;
@@ -724,6 +746,16 @@ int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
 }
 
 int coarse_pcg_partials_size() { return 2 * kPcgMaxCta; }
+
+int enforce_velocity_bcs(int nl, int nr, const double* coords, int bc_cmb, int bc_surf, double* const* v,
+                         cudaStream_t st)
+{
+    CompPtrs<double> p{};
+    for (int k = 0; k < 3; ++k) p.p[k] = v[k];
+    const int n = 10 * nl * nl;
+    enforce_bcs_kernel<<<(n + 127) / 128, 128, 0, st>>>(nl, nr, coords, bc_cmb, bc_surf, p);
+    return launch_status();
+}
 
 int coefficient_inject(int nlc, int nrc, const double* fine, double* coarse, bool reciprocal, cudaStream_t st)
 {

@@ -33,6 +33,23 @@ struct EddLaunch {
 template <typename T>
 int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream);
 
+// backward of the apply with respect to per-cell log-viscosity (adjoint.cu):
+// grad[cell] (+)= lambda_e^T A_e(kq0[cell]) u_e
+template <typename T>
+struct VjpLaunch {
+    int      nl = 0, nr = 0;
+    const T* coords = nullptr;
+    const T* radii  = nullptr;
+    const T* kq0    = nullptr;
+    const T* u[3]   = {nullptr, nullptr, nullptr};
+    const T* lam[3] = {nullptr, nullptr, nullptr};
+    T*       grad   = nullptr;  // (10, nl-1, nl-1, nr-1)
+    int      bc_cmb = 1, bc_surf = 1;
+    int      accumulate = 0;
+};
+template <typename T>
+int epsdivdiv_vjp_logeta(const VjpLaunch<T>& p, cudaStream_t stream);
+
 // ----------------------------------------------------------------------------
 // Coupling blocks and mass matrices (stokes_coupling.cu). All accumulate into
 // their outputs (callers zero them for Replace mode).

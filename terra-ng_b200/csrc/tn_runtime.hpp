@@ -199,6 +199,9 @@ struct EpsDivDivOp : Operator {
     void apply(void* const* src, void* const* dst, cudaStream_t st) override;
     template <typename T>
     void apply_t(const T* const* src, T* const* dst, cudaStream_t st);
+    // backward of the apply: grad_cell = d(lambda^T A u)/d log(eta_cell) (Q0 only)
+    template <typename T>
+    void vjp_logeta(const T* const* u, const T* const* lam, T* grad_cell, cudaStream_t st) const;
     // stored-matrix helpers
     void ensure_baked(bool need32, cudaStream_t st);
     void set_stored_matrices_from_coefficient(cudaStream_t st);  // element matrices of this level

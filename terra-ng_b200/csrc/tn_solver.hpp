@@ -131,6 +131,13 @@ class StokesSolver {
     bool solve(double* const* u, double* p, const double* const* fu, const double* fp, cudaStream_t st);
     // z = M^-1 v for 4-component vectors in the caller's layout
     void precondition_external(const double* const* v, double* const* z, cudaStream_t st);
+    // dJ/d log(eta_cell) of J = 1/2 sum over owned nodes |u - u_obs|^2 at the
+    // forward solution x (4 components): one adjoint solve K lambda = [u -
+    // u_obs; 0] (K is symmetric) and the backward kernel, grad = -lambda_u^T
+    // dA/dlog(eta) u. Needs a per-cell viscosity. lambda (4 components) is
+    // returned when not null. Returns whether the adjoint solve converged.
+    bool misfit_gradient(const double* const* x, const double* const* u_obs, double* grad_cell,
+                         double* const* lambda, cudaStream_t st);
 
     std::vector<double> history;  // relative residual estimates, history[0] = 1
     int                 iterations = 0;
@@ -141,6 +148,7 @@ class StokesSolver {
     const StokesOptions& options() const { return opt_; }
 
   private:
+    bool solve_internal(cudaStream_t st);  // x_ (initial guess -> solution), b_
     void precondition(const DVec<double>& v, DVec<double>& z, cudaStream_t st);
     void stokes_apply(const DVec<double>& x, DVec<double>& y, cudaStream_t st);
     void copy_in(DVec<double>& v, const double* const* u, const double* p, cudaStream_t st);
@@ -197,6 +205,9 @@ class VelocitySolver {
     DVec<double>                       x_, b_, r_, z_, p_, ap_;
     DVec<float>                        r32_, z32_;
 };
+
+int enforce_velocity_bcs(int nl, int nr, const double* coords, int bc_cmb, int bc_surf, double* const* v,
+                         cudaStream_t st);
 
 // coefficient of a coarser level: nodal injection (optionally reciprocal) or
 // the mean of the 8 child cells (solver_kernels.cu)

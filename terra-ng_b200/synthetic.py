@@ -8,6 +8,10 @@
   reference's SphericalHarmonicsTool).
 * temperature: a smooth field of the same kind (8 harmonics times sin(pi
   (r - r_min) / (r_max - r_min))) plus N(0, 0.01) noise drawn per unique node.
+* per-cell viscosity with blocks (adjoint workload): the smooth field above
+  evaluated at cell centres times seeded piecewise-constant lateral blocks
+  (tiles of each diamond, a seeded subset raised by a log-uniform factor in
+  [1, 10^4]), all radii.
 * buoyancy right-hand side f = M (T r_hat) with the vector mass matrix, then
   Dirichlet rows zeroed and free-slip normal components removed (the app's
   RHS assembly, apps/mantlecirculation/src/stokes_solver.hpp:650-671).
@@ -121,3 +125,53 @@ def enforce_boundary(shell: "T.Shell", level: int, f, bc_cmb: int, bc_surface: i
             dn = (f[..., side] * n).sum(0)
             f[..., side] -= dn[None] * n
     return f
+
+
+def cell_viscosity_blocks(shell: "T.Shell", level: int, seed: int = 3, tiles: int = 4, fraction: float = 0.3,
+                          max_log10: float = 4.0, background_log_amplitude: float = math.log(10.0)):
+    """Per-cell viscosity (10, nl-1, nl-1, nr-1): smooth background times lateral blocks."""
+    coords, radii = _geometry(shell, level)
+    nl, nr = coords.shape[1], radii.shape[0]
+    # cell centres: mean of the 4 corner unit vectors (normalised) and of the two radii
+    c = 0.25 * (coords[:, :-1, :-1] + coords[:, 1:, :-1] + coords[:, :-1, 1:] + coords[:, 1:, 1:])
+    c /= np.linalg.norm(c, axis=-1, keepdims=True)
+    rmid = 0.5 * (radii[:-1] + radii[1:])
+    s = _harmonic_sum(c, seed)
+    rad = np.cos(math.pi * (rmid - radii[0]) / (radii[-1] - radii[0]))
+    eta = np.exp(background_log_amplitude * s[..., None] * rad[None, None, None, :])
+    rng = np.random.default_rng(seed + 101)
+    t = max(1, min(tiles, nl - 1))
+    edge = (nl - 1) // t
+    for d in range(10):
+        for ix in range(t):
+            for iy in range(t):
+                if rng.uniform() < fraction:
+                    f = 10.0 ** rng.uniform(0.0, max_log10)
+                    eta[d, ix * edge:(ix + 1) * edge, iy * edge:(iy + 1) * edge, :] *= f
+    return eta
+
+
+def schur_coefficient_from_cells(shell: "T.Shell", velocity_level: int, eta_cell):
+    """Nodal 1/eta on the pressure level (velocity_level - 1) for a per-cell
+    viscosity: at each pressure node, the mean of 1/eta over the fine cells
+    touching it, averaged over all copies of an interface node."""
+    nlf = eta_cell.shape[1] + 1
+    nrf = eta_cell.shape[3] + 1
+    inv = 1.0 / eta_cell
+    acc = np.zeros((10, nlf, nlf, nrf))
+    cnt = np.zeros((10, nlf, nlf, nrf))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dr in (0, 1):
+                acc[:, dx:nlf - 1 + dx, dy:nlf - 1 + dy, dr:nrf - 1 + dr] += inv
+                cnt[:, dx:nlf - 1 + dx, dy:nlf - 1 + dy, dr:nrf - 1 + dr] += 1.0
+    cls, ncls = shell.duplicate_classes(velocity_level)
+    flat_a = acc.reshape(10 * nlf * nlf, nrf)
+    flat_c = cnt.reshape(10 * nlf * nlf, nrf)
+    cl = cls.reshape(-1)
+    for k in range(ncls):
+        m = np.where(cl == k)[0]
+        flat_a[m] = flat_a[m].sum(axis=0)
+        flat_c[m] = flat_c[m].sum(axis=0)
+    node = flat_a.reshape(acc.shape) / flat_c.reshape(cnt.shape)
+    return np.ascontiguousarray(node[:, ::2, ::2, ::2])

@@ -114,6 +114,8 @@ def load(path: str = LIB_PATH):
         "tn_solver_result": ([vp, ctypes.POINTER(i), dp, ctypes.POINTER(i)], i),
         "tn_solver_history": ([vp, dp, i, ctypes.POINTER(i)], i),
         "tn_solver_full_residual": ([vp, dp], i),
+        "tn_epsdivdiv_vjp": ([vp, vpp, vpp, vp, vpp, vp], i),
+        "tn_stokes_misfit_gradient": ([vp, vpp, vpp, vp, vpp, vp], i),
         "tn_solver_precondition": ([vp, vpp, vpp, vp], i),
         "tn_solver_vcycle": ([vp, i, vpp, vpp, vp], i),
         "tn_solver_level_lambda": ([vp, i, dp], i),
@@ -344,6 +346,13 @@ class EpsDivDiv(Operator):
     def set_tile(self, tile_y=0, chunk_x=0):
         _check(load().tn_operator_set_tile(self._h, tile_y, chunk_x))
 
+    def vjp(self, u, lam, grad_cell, grad_u=None, stream=None):
+        """Backward of apply: grad_cell = d(lam^T A u)/d log(eta_cell); grad_u = A lam (tn_epsdivdiv_vjp)."""
+        gu = None if grad_u is None else _ptrs(_comps(grad_u))
+        _check(load().tn_epsdivdiv_vjp(self._h, _ptrs(_comps(u)), _ptrs(_comps(lam)),
+                                       ctypes.c_void_p(grad_cell.data_ptr()), gu, _stream(stream)))
+        return grad_cell
+
     def set_stored_matrix_mode(self, mode=STORED_FULL, stream=None):
         _check(load().tn_operator_set_stored_matrix_mode(self._h, mode, _stream(stream)))
 
@@ -542,6 +551,17 @@ class StokesSolver(_Solver):
                                               _opt_ptr(k_schur), bc_cmb, bc_surface, ctypes.byref(self.options),
                                               _stream(stream), ctypes.byref(h)))
         self._h = h
+
+    def misfit_gradient(self, x, u_obs, grad_cell, lam=None, stream=None):
+        """dJ/dlog(eta_cell), J = 1/2 sum_owned |u - u_obs|^2 at the forward solution x (tn_stokes_misfit_gradient).
+        Returns whether the adjoint solve converged."""
+        lp = None if lam is None else _ptrs(_comps(lam))
+        rc = load().tn_stokes_misfit_gradient(self._h, _ptrs(_comps(x)), _ptrs(_comps(u_obs)),
+                                              ctypes.c_void_p(grad_cell.data_ptr()), lp, _stream(stream))
+        if rc == -7:
+            return False
+        _check(rc)
+        return True
 
 
 class VelocitySolver(_Solver):

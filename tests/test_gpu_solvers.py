@@ -203,7 +203,8 @@ def test_vcycle_fp32(cuda):
     import torch
 
     level, nlev = 4, 3
-    sh, k, g, solver, H = _hierarchy(level, nlev, (1, 2), 1, mixed_precision=1)
+    sh, k, g, solver, H = _hierarchy(level, nlev, (1, 2), 1, mixed_precision=1, coarse_relative_tolerance=1e-13,
+                                     coarse_max_iterations=3000)
     b = O.enforce_rhs_bcs(sh, consistent(sh, O.seeded_normal(sh.vec_shape, 33)), 1, 2)
     ref = H.multigrid().solve(np.zeros(sh.vec_shape), b)
     x = torch.zeros(sh.vec_shape, dtype=torch.float32, device=cuda)

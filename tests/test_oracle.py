@@ -117,3 +117,30 @@ def test_gca_galerkin_identity():
     assert np.abs(m - np.transpose(m, (0, 2, 1))).max() <= 1e-12 * np.abs(m).max()
     ev = np.linalg.eigvalsh(m[:50])
     assert ev.min() > -1e-10 * ev.max()
+
+
+@pytest.mark.parametrize("bcs", [(1, 1), (1, 2), (2, 2), (0, 0)])
+def test_vjp_logeta_matches_finite_differences(bcs):
+    """g_e = lambda^T dA/dlog(eta_e) u against central differences of
+    lambda^T A(exp(theta)) u (A is linear in eta_e, so the difference
+    quotient is exact up to rounding)."""
+    sh = O.Shell(2)
+    rng = np.random.default_rng(60)
+    theta = rng.uniform(-2.0, 2.0, size=sh.cell_shape)
+    u = consistent(sh, O.seeded_normal(sh.vec_shape, 61))
+    lam = consistent(sh, O.seeded_normal(sh.vec_shape, 62))
+    op = O.EpsDivDiv(sh, k_q0=np.exp(theta), bc_cmb=bcs[0], bc_surface=bcs[1])
+    g = op.vjp_logeta(u, lam)
+
+    def J(th):
+        return float(np.sum(lam * O.EpsDivDiv(sh, k_q0=np.exp(th), bc_cmb=bcs[0], bc_surface=bcs[1]).apply(
+            u, path="slow", comm=False)))
+
+    h = 1e-6
+    for _ in range(6):
+        e = tuple(rng.integers(0, n) for n in sh.cell_shape)
+        tp, tm = theta.copy(), theta.copy()
+        tp[e] += h
+        tm[e] -= h
+        fd = (J(tp) - J(tm)) / (2 * h)
+        assert abs(fd - g[e]) <= 1e-6 * max(abs(g[e]), 1e-3 * np.abs(g).max())

@@ -224,8 +224,10 @@ typedef struct tn_solver_options {
     uint64_t seed;                      /* power-iteration start vectors (12345) */
     int      normalize_pressure;        /* Stokes: subtract the owned-node pressure mean after the solve, as
                                            StokesContext::solve does (stokes_solver.hpp:684-690) (1) */
-    int      project_pressure_mean;     /* Stokes: iterate on P K, P removing the pressure mean, i.e. treat
+    int      project_pressure_mean;     /* Stokes: iterate on P K P, P removing the pressure mean, i.e. treat
                                            constant pressure as a null vector; not in the reference (0) */
+    int      cuda_graphs;               /* Stokes: capture each Arnoldi step once and replay it as a CUDA
+                                           graph (1) */
 } tn_solver_options;
 void tn_solver_options_default(tn_solver_options* opts);
 /* Stokes solve on velocity_level / velocity_level-1 (StokesContext,

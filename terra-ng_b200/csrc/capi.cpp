@@ -639,6 +639,7 @@ void tn_solver_options_default(tn_solver_options* o)
     o->seed                      = 12345;
     o->normalize_pressure        = 1;
     o->project_pressure_mean     = 0;
+    o->cuda_graphs               = 1;
 }
 
 int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,
@@ -659,6 +660,7 @@ int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* e
         so.mg       = mg_options(o);
         so.normalize_pressure    = o.normalize_pressure != 0;
         so.project_pressure_mean = o.project_pressure_mean != 0;
+        so.use_graphs            = o.cuda_graphs != 0;
         auto s      = std::make_unique<tn_solver>();
         s->shell    = shell;
         s->stokes   = std::make_unique<tn::StokesSolver>(shell->impl.get(), velocity_level, eta_nodal_dev,

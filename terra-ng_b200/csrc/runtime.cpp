@@ -56,6 +56,15 @@ std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, 
             }
             dl->canon_lat = upload(canon);
         }
+        if (h.nl > 1) {
+            const size_t ncol = static_cast<size_t>(10) * (h.nl - 1) * (h.nl - 1) * 20;
+            dl->colgeo64.alloc(ncol * sizeof(double));
+            dl->colgeo32.alloc(ncol * sizeof(float));
+            if (column_geometry_table<double>(h.nl, dl->coords64.as<double>(), dl->colgeo64.as<double>(), nullptr) != 0 ||
+                column_geometry_table<float>(h.nl, dl->coords32.as<float>(), dl->colgeo32.as<float>(), nullptr) != 0)
+                throw Error(kErrCuda, "column geometry launch failed");
+            cuda_check(cudaDeviceSynchronize(), "column geometry");
+        }
         dl->iface.num_classes = static_cast<int>(h.dup_offset.size()) - 1;
         dl->iface.offset      = dl->dup_offset.as<int32_t>();
         dl->iface.members     = dl->dup_members.as<int32_t>();
@@ -245,11 +254,15 @@ void DivergenceOp::apply_t(const T* const* src, T* p, cudaStream_t st) const
     c.nl     = L.nl();
     c.nr     = L.nr();
     c.coords = L.coords<T>();
+    c.colgeo = L.colgeo<T>();
     c.radii  = L.radii<T>();
     c.bc_cmb = bc_cmb;
     c.bc_surf = bc_surf;
     for (int k = 0; k < 3; ++k) c.u[k] = src[k];
     c.p_out = p;
+    const size_t need = sizeof(T) * 2 * static_cast<size_t>(L.cells());
+    if (scratch.size() < need) scratch.alloc(need);
+    c.wedge_scratch = scratch.as<T>();
     if (divergence_apply<T>(c, st) != 0) throw Error(kErrCuda, "divergence launch failed");
     if (comm_mode == 1) iface<T>(Lc, 1, &p, st);
 }
@@ -267,12 +280,16 @@ void GradientOp::apply_t(const T* p, T* const* dst, cudaStream_t st) const
 {
     const DeviceLevel& L = lvl();
     if (level < 1) throw Error(kErrArg, "gradient needs a coarser pressure level");
-    if (apply_mode == 0) zero_components<T>(L.nodes(), 3, dst, st);
     CouplingLaunch<T> c;
     c.nl      = L.nl();
     c.nr      = L.nr();
     c.coords  = L.coords<T>();
+    c.colgeo  = L.colgeo<T>();
     c.radii   = L.radii<T>();
+    c.add     = apply_mode == 1 ? 1 : 0;
+    const size_t need = sizeof(T) * 2 * static_cast<size_t>(L.cells());
+    if (scratch.size() < need) scratch.alloc(need);
+    c.wedge_scratch = scratch.as<T>();
     c.bc_cmb  = bc_cmb;
     c.bc_surf = bc_surf;
     c.p_in    = p;

@@ -188,6 +188,7 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     // the coarsest CG runs over stored matrices
     if (!ops64_[0]->stored) ops64_[0]->set_stored_matrices_from_coefficient(st);
     ops64_[0]->ensure_baked(false, st);
+    chk(coarse_pcg_prepare(sh->level(0).nl(), sh->level(0).nr()), "coarse CG configuration");
 
     // FP32 operators where the apply is matrix-free
     if (o.fp32) {
@@ -250,6 +251,9 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     }
     // Chebyshev spectrum estimates (chebyshev.hpp estimate_max_eigenvalues)
     for (int l = 1; l <= fine_; ++l) lambda_[l] = power_iteration(l, o.power_iters, o.seed + 7919ull * l, st);
+    // one FP32 apply per level now: kernel attributes are set outside any later graph capture
+    if (o.fp32)
+        for (int l = 1; l <= fine_; ++l) apply<float>(l, w32_.e[l].data(), w32_.tmp[l].data(), st);
 
     // coarsest CG vectors
     const VecDesc v0 = velocity_desc(sh->level(0));
@@ -542,6 +546,14 @@ StokesSolver::StokesSolver(const Shell* sh, int vlevel, const double* eta_nodal,
         t32_.alloc(velocity_desc(Lu));
         z32_.alloc(velocity_desc(Lu));
     }
+    // everything an Arnoldi step touches is allocated here, so that the step can be captured
+    const size_t wedges = sizeof(double) * 2 * static_cast<size_t>(Lu.cells());
+    K_.B.scratch.alloc(wedges);
+    K_.BT.scratch.alloc(wedges);
+    BT_.scratch.alloc(wedges);
+    graphs_.assign(o.restart, nullptr);
+    graph_kernels_.assign(o.restart, 0);
+    cuda_check(cudaStreamCreateWithFlags(&ws_, cudaStreamNonBlocking), "create stream");
     cuda_check(cudaStreamSynchronize(st), "synchronize");
 }
 
@@ -629,17 +641,22 @@ void StokesSolver::precondition_external(const double* const* v, double* const* 
 
 bool StokesSolver::solve(double* const* u, double* p, const double* const* fu, const double* fp, cudaStream_t st)
 {
-    copy_in(x_, u, p, st);
-    copy_in(b_, fu, fp, st);
-    const bool ok = solve_internal(st);
-    copy_out(x_, u, p, st);
+    // the caller's producers first, then everything on the solver's own stream
+    // (graph capture needs a stream other than the legacy default stream)
     cuda_check(cudaStreamSynchronize(st), "synchronize");
+    copy_in(x_, u, p, ws_);
+    copy_in(b_, fu, fp, ws_);
+    const bool ok = solve_internal(ws_);
+    copy_out(x_, u, p, ws_);
+    cuda_check(cudaStreamSynchronize(ws_), "synchronize");
     return ok;
 }
 
 bool StokesSolver::misfit_gradient(const double* const* x, const double* const* u_obs, double* grad_cell,
-                                   double* const* lambda, cudaStream_t st)
+                                   double* const* lambda, cudaStream_t caller)
 {
+    cuda_check(cudaStreamSynchronize(caller), "synchronize");
+    cudaStream_t st = ws_;
     if (!K_.A.q0) throw Error(kErrUnsupported, "the log-viscosity gradient needs a per-cell viscosity");
     const DeviceLevel& Lu = sh_->level(vlevel_);
     const size_t       bu = sizeof(double) * Lu.nodes();
@@ -679,6 +696,72 @@ bool StokesSolver::misfit_gradient(const double* const* x, const double* const* 
     return ok;
 }
 
+// Device work of Arnoldi step j without any host synchronisation:
+// V_j = w / h_{j,j-1} (j > 0), Z_j = M^-1 V_j, w = K Z_j, Gram-Schmidt of w
+// against V_0..V_j and its norm into the scalar slots. With CUDA graphs on,
+// each j is captured once (its pointers are fixed) and replayed.
+void StokesSolver::step_body(int j, cudaStream_t st)
+{
+    const int64_t nt = blk_.total;
+    if (j > 0) chk(scale_by_recip<double>(nt, V_[j].data(), w_.data(), scratch_.s(kH0 + j), st), "scale");
+    DVec<double>& Zj = Z_[j];
+    cuda_check(cudaMemsetAsync(Zj.data(), 0, sizeof(double) * nt, st), "zero");
+    precondition(V_[j], Zj, st);
+    if (opt_.project_pressure_mean) remove_pressure_mean(Zj, kProj, st);
+    arnoldi_tail(j, st);
+}
+
+void StokesSolver::arnoldi_tail(int j, cudaStream_t st)
+{
+    stokes_apply(Z_[j], w_, st);
+    if (opt_.project_pressure_mean) remove_pressure_mean(w_, kProj, st);
+    for (int i = 0; i <= j; ++i)
+        chk(mgs_step(blk_, w_.data(), i > 0 ? V_[i - 1].data() : nullptr, scratch_.s(kH0 + i - 1), V_[i].data(),
+                     scratch_.s(kH0 + i), scratch_.rs(), st),
+            "gram-schmidt");
+    chk(mgs_step(blk_, w_.data(), V_[j].data(), scratch_.s(kH0 + j), nullptr, scratch_.s(kH0 + j + 1), scratch_.rs(),
+                 st),
+        "gram-schmidt");
+}
+
+void StokesSolver::run_step(int j, cudaStream_t st)
+{
+    if (!opt_.use_graphs) {
+        step_body(j, st);
+        return;
+    }
+    if (graphs_[j] == nullptr) {
+        cudaGraph_t    g  = nullptr;
+        const uint64_t l0 = launch_count();
+        cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            step_body(j, st);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(st, &g), "end capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e  = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        cuda_check(e, "instantiate graph");
+        graphs_[j]        = exec;
+        graph_kernels_[j] = static_cast<int>(launch_count() - l0);
+        note_launch(-graph_kernels_[j]);  // counted again below, when they run
+    }
+    cuda_check(cudaGraphLaunch(graphs_[j], st), "graph launch");
+    note_launch(graph_kernels_[j]);
+}
+
+StokesSolver::~StokesSolver()
+{
+    for (auto& g : graphs_)
+        if (g) cudaGraphExecDestroy(g);
+    if (ws_) cudaStreamDestroy(ws_);
+}
+
 bool StokesSolver::solve_internal(cudaStream_t st)
 {
     const double eps   = std::numeric_limits<double>::epsilon();
@@ -699,12 +782,13 @@ bool StokesSolver::solve_internal(cudaStream_t st)
     // floors at an O(h^2) level. full_relres reports the unprojected residual.
     const double one_m[2] = {1.0, -1.0};
     const int    kFull    = Scratch::kScalars - 2;  // scalar slots away from the Hessenberg column
+    static_assert(Scratch::kScalars - 1 == kProj, "projection scratch slot");
     auto residual = [&](bool report_full) {  // r = b - K x, returns ||r|| (projected when enabled)
         stokes_apply(x_, r_, st);
         lin<double>(nt, r_.data(), 0.0, 2, one_m, b_.data(), r_.data(), st);
         if (report_full)
             chk(vec_dot<double>(blk_, r_.data(), r_.data(), scratch_.s(kFull), scratch_.rs(), true, st), "norm");
-        if (opt_.project_pressure_mean) remove_pressure_mean(r_, kFull + 1, st);
+        if (opt_.project_pressure_mean) remove_pressure_mean(r_, kProj, st);
         chk(vec_dot<double>(blk_, r_.data(), r_.data(), scratch_.s(0), scratch_.rs(), true, st), "norm");
         scratch_.fetch(Scratch::kScalars, st);
         return scratch_.host[0];
@@ -712,7 +796,7 @@ bool StokesSolver::solve_internal(cudaStream_t st)
     // the iterate's pressure stays mean-free under the projection, so the
     // iteration is on [A, B^T P; P B, 0] over mean-free pressures, which is
     // symmetric and nonsingular (the solution is a function of the data)
-    if (opt_.project_pressure_mean) remove_pressure_mean(x_, kFull + 1, st);
+    if (opt_.project_pressure_mean) remove_pressure_mean(x_, kProj, st);
     double       beta0 = residual(true);
     const double init_full = scratch_.host[kFull];
     const double init  = beta0;
@@ -725,7 +809,7 @@ bool StokesSolver::solve_internal(cudaStream_t st)
     std::vector<double> H((m + 1) * m), g(m + 1), cs(m + 1), sn(m + 1), y(m);
     auto                h = [&](int i, int j) -> double& { return H[i * m + j]; };
     int                 total = 0, steps = 0;
-    const int           H0    = 2;  // device scalar slots: s(0) norm scratch, s(H0 + i) Hessenberg column
+    const int           H0    = kH0;  // device scalar slots: s(0) norm scratch, s(H0 + i) Hessenberg column
     while (total < opt_.max_iter) {
         chk(scale_by_recip<double>(nt, V_[0].data(), r_.data(), scratch_.s(0), st), "scale");
         std::fill(H.begin(), H.end(), 0.0);
@@ -737,25 +821,15 @@ bool StokesSolver::solve_internal(cudaStream_t st)
         for (int j = 0; j < m && total < opt_.max_iter; ++j, ++total) {
             DVec<double>& Zj = Z_[j];
             ++steps;
-            cuda_check(cudaMemsetAsync(Zj.data(), 0, sizeof(double) * nt, st), "zero");
-            precondition(V_[j], Zj, st);
-            if (opt_.project_pressure_mean) remove_pressure_mean(Zj, kFull + 1, st);
-            for (int attempt = 0; attempt < 2; ++attempt) {
-                stokes_apply(Zj, w_, st);
-                if (opt_.project_pressure_mean) remove_pressure_mean(w_, kFull + 1, st);
-                for (int i = 0; i <= j; ++i)
-                    chk(mgs_step(blk_, w_.data(), i > 0 ? V_[i - 1].data() : nullptr, scratch_.s(H0 + i - 1),
-                                 V_[i].data(), scratch_.s(H0 + i), scratch_.rs(), st),
-                        "gram-schmidt");
-                chk(mgs_step(blk_, w_.data(), V_[j].data(), scratch_.s(H0 + j), nullptr, scratch_.s(H0 + j + 1),
-                             scratch_.rs(), st),
-                    "gram-schmidt");
-                scratch_.fetch(H0 + j + 2, st);
-                if (scratch_.host_flag() == 0 || attempt == 1) break;
+            run_step(j, st);
+            scratch_.fetch(H0 + j + 2, st);
+            if (scratch_.host_flag() != 0) {
                 // the preconditioner produced NaN/Inf: keep its input instead (fgmres.hpp:191-210)
                 cuda_check(cudaMemsetAsync(scratch_.flag_dev(), 0, sizeof(int), st), "zero flag");
                 cuda_check(cudaMemcpyAsync(Zj.data(), V_[j].data(), sizeof(double) * nt, cudaMemcpyDeviceToDevice, st),
                            "copy");
+                arnoldi_tail(j, st);
+                scratch_.fetch(H0 + j + 2, st);
             }
             for (int i = 0; i <= j; ++i) h(i, j) = scratch_.host[H0 + i];
             const double hj1 = scratch_.host[H0 + j + 1];
@@ -764,8 +838,7 @@ bool StokesSolver::solve_internal(cudaStream_t st)
                 inner       = j + 1;
                 break;
             }
-            h(j + 1, j) = hj1;
-            if (hj1 > 0.0) chk(scale_by_recip<double>(nt, V_[j + 1].data(), w_.data(), scratch_.s(H0 + j + 1), st), "scale");
+            h(j + 1, j) = hj1;  // V_{j+1} = w / h_{j+1,j} opens the next step
             for (int i = 0; i < j; ++i) {
                 const double t = cs[i] * h(i, j) + sn[i] * h(i + 1, j);
                 h(i + 1, j)    = -sn[i] * h(i, j) + cs[i] * h(i + 1, j);

@@ -14,6 +14,8 @@
 //   cluster synchronise with the hardware cluster barrier, so the whole solve is
 //   one launch.
 #include <cfloat>
+#include <map>
+#include <mutex>
 
 #include "tn_device.cuh"
 #include "tn_kernels.hpp"
@@ -689,51 +691,78 @@ int pcg_cluster_size(size_t smem)
 
 int coarse_pcg_cluster_size() { return pcg_cluster_size(0); }
 
-int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
+namespace {
+struct PcgConfig {
+    int    cs = 0, cpc = 0, in_smem = 0;
+    size_t node_bytes = 0, smem = 0;
+};
+
+// Launch configuration for a coarsest level of nc cells, decided once per nc
+// (function attributes and occupancy queries stay out of launches, so the
+// launch can be captured in a CUDA graph).
+int pcg_config(int nc, PcgConfig& out)
 {
-    constexpr size_t kSmemLimit = 200 * 1024;
-    CoarsePcgArgs    args       = args_in;
-    const int        nc         = 10 * (args.nl - 1) * (args.nl - 1) * (args.nr - 1);
-    // cluster size first from the node table alone, then decide on matrix residency
-    int       cs  = 8;
-    int       cpc = (nc + kPcgMaxCta - 1) / kPcgMaxCta;
-    size_t    node_bytes = (static_cast<size_t>(48) * cpc + 15) / 16 * 16;
-    size_t    smem       = node_bytes + static_cast<size_t>(342 * 8) * cpc;
-    bool      in_smem    = smem <= kSmemLimit;
-    if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(in_smem ? smem : node_bytes)) != cudaSuccess) {
-        cudaGetLastError();
-        return -2;
+    static std::mutex                  mu;
+    static std::map<int, PcgConfig>    cache;
+    static size_t                      configured = 0;
+    std::lock_guard<std::mutex>        lock(mu);
+    auto                               it = cache.find(nc);
+    if (it != cache.end()) {
+        out = it->second;
+        return 0;
     }
-    cs = pcg_cluster_size(in_smem ? smem : node_bytes);
-    if (cs != kPcgMaxCta) {
-        cpc        = (nc + cs - 1) / cs;
-        node_bytes = (static_cast<size_t>(48) * cpc + 15) / 16 * 16;
-        smem       = node_bytes + static_cast<size_t>(342 * 8) * cpc;
-        in_smem    = smem <= kSmemLimit;
-        if (!in_smem) smem = node_bytes;
-        if (node_bytes > kSmemLimit) return -1;
+    constexpr size_t kSmemLimit = 200 * 1024;
+    PcgConfig        c;
+    auto             layout = [&](int cs) {
+        c.cs         = cs;
+        c.cpc        = (nc + cs - 1) / cs;
+        c.node_bytes = (static_cast<size_t>(48) * c.cpc + 15) / 16 * 16;
+        c.smem       = c.node_bytes + static_cast<size_t>(342 * 8) * c.cpc;
+        c.in_smem    = c.smem <= kSmemLimit ? 1 : 0;
+        if (!c.in_smem) c.smem = c.node_bytes;
+    };
+    layout(kPcgMaxCta);
+    if (c.smem > configured) {
         if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)) != cudaSuccess) {
+                                 static_cast<int>(kSmemLimit)) != cudaSuccess) {
             cudaGetLastError();
             return -2;
         }
-    } else if (!in_smem) {
-        smem = node_bytes;
-        if (node_bytes > kSmemLimit) return -1;
+        configured = kSmemLimit;
     }
-    args.cells_per_cta = cpc;
-    args.node_bytes    = static_cast<int>(node_bytes);
-    args.mats_in_smem  = in_smem ? 1 : 0;
+    if (pcg_cluster_size(c.smem) != kPcgMaxCta) layout(8);
+    if (c.node_bytes > kSmemLimit) return -1;
+    cache[nc] = c;
+    out       = c;
+    return 0;
+}
+}  // namespace
+
+int coarse_pcg_prepare(int nl, int nr)
+{
+    PcgConfig c;
+    return pcg_config(10 * (nl - 1) * (nl - 1) * (nr - 1), c);
+}
+
+int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
+{
+    CoarsePcgArgs args = args_in;
+    const int     nc   = 10 * (args.nl - 1) * (args.nl - 1) * (args.nr - 1);
+    PcgConfig     c;
+    const int     rc = pcg_config(nc, c);
+    if (rc != 0) return rc;
+    args.cells_per_cta = c.cpc;
+    args.node_bytes    = static_cast<int>(c.node_bytes);
+    args.mats_in_smem  = c.in_smem;
     cudaLaunchConfig_t  cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id               = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.x = c.cs;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
-    cfg.gridDim            = dim3(cs);
+    cfg.gridDim            = dim3(c.cs);
     cfg.blockDim           = dim3(kPcgThreads);
-    cfg.dynamicSmemBytes   = smem;
+    cfg.dynamicSmemBytes   = c.smem;
     cfg.stream             = st;
     cfg.attrs              = at;
     cfg.numAttrs           = 1;

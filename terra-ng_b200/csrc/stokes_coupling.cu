@@ -60,6 +60,7 @@ template <typename T>
 struct CouplingArgs {
     int      nl, nr;  // fine level
     const T* coords;  // fine unit-sphere coords
+    const T* colgeo;  // fine per-column wedge geometry (20 values per column)
     const T* radii;   // fine radii
     int      bc_cmb, bc_surf;
     const T* u[3];    // fine velocity (divergence input / gradient output)
@@ -103,92 +104,210 @@ __device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int 
     n[2]       = c[2];
 }
 
+// Both blocks go through one scalar per fine wedge, stored in a scratch array
+// wedge_val[2 * fine_cell + w]:
+//   B  : -|det J_w| div_w(u), div_w = tr(G) = e1.a + e2.b + e3.D (the
+//        factorised velocity gradient of the epsilon-div-div kernel);
+//   B^T: -|det J_w| p_interp,w with p_interp the coarse-pressure interpolation
+//        at the fine wedge's centroid.
+// Pass 1 runs one thread per fine cell (r fastest); pass 2 distributes:
+// B adds the 16 fine wedges of a coarse cell into its 8 corners (8 atomics per
+// coarse cell), B^T gathers, per fine node, the up to 12 wedges around it
+// (no atomics, every node written once).
+
 template <typename T>
-__global__ void divergence_kernel(CouplingArgs<T> A)
+__device__ __forceinline__ void decode_cell(int cell, int nl, int nr, int& d, int& x, int& y, int& r)
 {
-    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int r  = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y  = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
-    if (r >= nr - 1) return;
-    T g[2][6][3], adet[2];
-    cell_grads<T>(A.coords, nl, d, x, y, A.radii[r], A.radii[r + 1], g, adet);
+    r     = cell % (nr - 1);
+    int t = cell / (nr - 1);
+    y     = t % (nl - 1);
+    t /= (nl - 1);
+    x = t % (nl - 1);
+    d = t / (nl - 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
+{
+    const int nl = A.nl, nr = A.nr;
+    const int nc   = 10 * (nl - 1) * (nl - 1) * (nr - 1);
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= nc) return;
+    int d, x, y, r;
+    decode_cell<T>(cell, nl, nr, d, x, y, r);
+    const T*   G  = A.colgeo + static_cast<int64_t>(cell / (nr - 1)) * 20;
+    const T    r0 = A.radii[r], r1 = A.radii[r + 1];
+    const T    rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+    const T    alpha = T(0.5) / rm, beta = T(1) / (T(6) * hdr);
     const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
     const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
     const int  bside  = at_cmb ? 0 : 1;
-    const int  frw    = r & 1;
+    // corner values u[q][s][c] with the boundary treatment of the wedge nodes
+    T u[4][2][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int qx = x + (q & 1), qy = y + (q >> 1);
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+            const int64_t id = node_index(nl, nr, d, qx, qy, r + s2);
+            T             v0 = A.u[0][id], v1 = A.u[1][id], v2 = A.u[2][id];
+            if ((at_cmb || at_surf) && s2 == bside) {
+                if (bcf == 1) {
+                    v0 = v1 = v2 = T(0);
+                } else if (bcf == 2) {
+                    T nn[3];
+                    unit_normal<T>(A.coords, nl, d, qx, qy, nn);
+                    const T un = v0 * nn[0] + v1 * nn[1] + v2 * nn[2];
+                    v0 -= un * nn[0];
+                    v1 -= un * nn[1];
+                    v2 -= un * nn[2];
+                }
+            }
+            u[q][s2][0] = v0;
+            u[q][s2][1] = v1;
+            u[q][s2][2] = v2;
+        }
+    }
 #pragma unroll
     for (int w = 0; w < 2; ++w) {
-        T div = T(0);
+        const T*  gw = G + 10 * w;
+        const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
+        T         div = T(0);
 #pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            const int  nx = x + woff(w, n, 0), ny = y + woff(w, n, 1), nrr = r + woff(w, n, 2);
-            const bool bn = (at_cmb || at_surf) && (woff(w, n, 2) == bside);
-            if (bcf == 1 && bn) continue;
-            const int64_t id = node_index(nl, nr, d, nx, ny, nrr);
-            T             u0 = A.u[0][id], u1 = A.u[1][id], u2 = A.u[2][id];
-            if (bcf == 2 && bn) {
-                T nn[3];
-                unit_normal<T>(A.coords, nl, d, nx, ny, nn);
-                const T un = u0 * nn[0] + u1 * nn[1] + u2 * nn[2];
-                u0 -= un * nn[0];
-                u1 -= un * nn[1];
-                u2 -= un * nn[2];
-            }
-            div += g[w][n][0] * u0 + g[w][n][1] * u1 + g[w][n][2] * u2;
+        for (int c = 0; c < 3; ++c) {
+            const T S0 = u[q0][0][c] + u[q0][1][c], S1 = u[q1][0][c] + u[q1][1][c], S2 = u[q2][0][c] + u[q2][1][c];
+            const T Dc = (u[q0][1][c] - u[q0][0][c]) + (u[q1][1][c] - u[q1][0][c]) + (u[q2][1][c] - u[q2][0][c]);
+            div += alpha * (gw[c] * (S1 - S0) + gw[3 + c] * (S2 - S0)) + beta * gw[6 + c] * Dc;
         }
-        const T   pre = -adet[w] * div;
-        const int flw = fine_lat_wedge(x, y, w);
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-            const int64_t id =
-                node_index(nlc, nrc, d, x / 2 + woff(w, i, 0), y / 2 + woff(w, i, 1), r / 2 + woff(w, i, 2));
-            atomicAdd(&A.po[id], pre * shape_coarse_centroid<T>(i, frw, flw));
-        }
+        wv[2 * static_cast<int64_t>(cell) + w] = -(gw[9] * rm * rm * hdr) * div;
     }
 }
 
 template <typename T>
-__global__ void gradient_kernel(CouplingArgs<T> A)
+__global__ void __launch_bounds__(128) div_scatter_kernel(CouplingArgs<T> A, const T* __restrict__ wv)
 {
     const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int r  = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y  = blockIdx.y % (nl - 1), x = blockIdx.y / (nl - 1), d = blockIdx.z;
-    if (r >= nr - 1) return;
-    T g[2][6][3], adet[2];
-    cell_grads<T>(A.coords, nl, d, x, y, A.radii[r], A.radii[r + 1], g, adet);
-    const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
-    const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
-    const int  bside  = at_cmb ? 0 : 1;
-    const int  frw    = r & 1;
+    const int ncc  = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= ncc) return;
+    int d, X, Y, R;
+    decode_cell<T>(cell, nlc, nrc, d, X, Y, R);
+    T acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+        const int     x = 2 * X + (f & 1), y = 2 * Y + ((f >> 1) & 1), c = f >> 2, r = 2 * R + c;
+        const int64_t fc = node_index(nl - 1, nr - 1, d, x, y, r);
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const T   pre = wv[2 * fc + w];
+            const int flw = fine_lat_wedge(x, y, w);
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                acc[woff(w, i, 0) + 2 * woff(w, i, 1) + 4 * woff(w, i, 2)] += pre * shape_coarse_centroid<T>(i, c, flw);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        atomicAdd(&A.po[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))], acc[k]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) grad_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
+{
+    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    const int nc   = 10 * (nl - 1) * (nl - 1) * (nr - 1);
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= nc) return;
+    int d, x, y, r;
+    decode_cell<T>(cell, nl, nr, d, x, y, r);
+    const T* G  = A.colgeo + static_cast<int64_t>(cell / (nr - 1)) * 20;
+    const T  r0 = A.radii[r], r1 = A.radii[r + 1];
+    const T  rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+    const int X = x / 2, Y = y / 2, R = r / 2, frw = r & 1;
+    T         pc[8];  // coarse cell corner pressures
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pc[k] = A.p[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))];
 #pragma unroll
     for (int w = 0; w < 2; ++w) {
         const int flw = fine_lat_wedge(x, y, w);
         T         pi  = T(0);
 #pragma unroll
         for (int j = 0; j < 6; ++j)
-            pi += shape_coarse_centroid<T>(j, frw, flw) *
-                  A.p[node_index(nlc, nrc, d, x / 2 + woff(w, j, 0), y / 2 + woff(w, j, 1), r / 2 + woff(w, j, 2))];
-        const T pre = -adet[w] * pi;
+            pi += shape_coarse_centroid<T>(j, frw, flw) * pc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)];
+        wv[2 * static_cast<int64_t>(cell) + w] = -(G[10 * w + 9] * rm * rm * hdr) * pi;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) grad_gather_kernel(CouplingArgs<T> A, const T* __restrict__ wv, int add)
+{
+    const int     nl = A.nl, nr = A.nr;
+    const int64_t nn_total = 10ll * nl * nl * nr;
+    const int64_t node     = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (node >= nn_total) return;
+    const int r = static_cast<int>(node % nr);
+    int64_t   t = node / nr;
+    const int y = static_cast<int>(t % nl);
+    t /= nl;
+    const int  x = static_cast<int>(t % nl);
+    const int  d = static_cast<int>(t / nl);
+    const bool on_cmb = r == 0, on_surf = r == nr - 1;
+    const int  bcn    = on_cmb ? A.bc_cmb : (on_surf ? A.bc_surf : 0);
+    T          o[3]   = {T(0), T(0), T(0)};
+    if (bcn != 1) {
 #pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            const int  nx = x + woff(w, n, 0), ny = y + woff(w, n, 1), nrr = r + woff(w, n, 2);
-            const bool bn = (at_cmb || at_surf) && (woff(w, n, 2) == bside);
-            if (bcf == 1 && bn) continue;
-            T c0 = pre * g[w][n][0], c1 = pre * g[w][n][1], c2 = pre * g[w][n][2];
-            if (bcf == 2 && bn) {
-                T nn[3];
-                unit_normal<T>(A.coords, nl, d, nx, ny, nn);
-                const T cn = c0 * nn[0] + c1 * nn[1] + c2 * nn[2];
-                c0 -= cn * nn[0];
-                c1 -= cn * nn[1];
-                c2 -= cn * nn[2];
+        for (int ab = 0; ab < 4; ++ab) {
+            const int a = ab & 1, b = ab >> 1;
+            const int xc = x - a, yc = y - b;
+            if (xc < 0 || yc < 0 || xc > nl - 2 || yc > nl - 2) continue;
+            const T*  G = A.colgeo + ((static_cast<int64_t>(d) * (nl - 1) + xc) * (nl - 1) + yc) * 20;
+            const int q = a + 2 * b;  // hex corner of the node in the cell
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int rc = r - c;
+                if (rc < 0 || rc > nr - 2) continue;
+                const T       r0 = A.radii[rc], r1 = A.radii[rc + 1];
+                const T       rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+                const T       alpha = T(0.5) / rm, sb = (c == 0 ? T(-1) : T(1)) / (T(6) * hdr);
+                const int64_t fc    = node_index(nl - 1, nr - 1, d, xc, yc, rc);
+#pragma unroll
+                for (int w = 0; w < 2; ++w) {
+                    const int m = w == 0 ? q : 3 - q;  // lateral index of corner q in wedge w
+                    if (m > 2) continue;
+                    const T* gw  = G + 10 * w;
+                    const T  pre = wv[2 * fc + w];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
+                        o[i] += pre * (alpha * L + sb * gw[6 + i]);
+                    }
+                }
             }
-            const int64_t id = node_index(nl, nr, d, nx, ny, nrr);
-            atomicAdd(&A.uo[0][id], c0);
-            atomicAdd(&A.uo[1][id], c1);
-            atomicAdd(&A.uo[2][id], c2);
+        }
+        if (bcn == 2) {
+            T nv[3];
+            unit_normal<T>(A.coords, nl, d, x, y, nv);
+            const T on = o[0] * nv[0] + o[1] * nv[1] + o[2] * nv[2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) o[i] -= on * nv[i];
         }
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) A.uo[i][node] = add ? A.uo[i][node] + o[i] : o[i];
+}
+
+// Per-column wedge geometry table (column_geometry, 20 values per column).
+template <typename T>
+__global__ void colgeo_kernel(int nl, const T* coords, T* out)
+{
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= 10 * (nl - 1) * (nl - 1)) return;
+    const int y = col % (nl - 1);
+    const int x = (col / (nl - 1)) % (nl - 1);
+    const int d = col / ((nl - 1) * (nl - 1));
+    column_geometry<T>(coords, nl, d, x, y, out + static_cast<int64_t>(col) * 20);
 }
 
 // Felippa 3x2 rule (quadrature.hpp:57-100).
@@ -295,36 +414,55 @@ inline dim3 cell_grid(int nl, int nr, int threads) { return dim3((nr - 1 + threa
 }  // namespace
 
 template <typename T>
-int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t st)
+static CouplingArgs<T> coupling_args(const CouplingLaunch<T>& p)
 {
     CouplingArgs<T> a{};
-    a.nl = p.nl;
-    a.nr = p.nr;
-    a.coords = p.coords;
-    a.radii  = p.radii;
-    a.bc_cmb = p.bc_cmb;
+    a.nl      = p.nl;
+    a.nr      = p.nr;
+    a.coords  = p.coords;
+    a.colgeo  = p.colgeo;
+    a.radii   = p.radii;
+    a.bc_cmb  = p.bc_cmb;
     a.bc_surf = p.bc_surf;
-    for (int c = 0; c < 3; ++c) a.u[c] = p.u[c];
-    a.po             = p.p_out;
-    const int thr    = p.nr - 1 >= 64 ? 64 : 32;
-    divergence_kernel<T><<<cell_grid(p.nl, p.nr, thr), thr, 0, st>>>(a);
-    return launch_status();
+    for (int c = 0; c < 3; ++c) {
+        a.u[c]  = p.u[c];
+        a.uo[c] = p.u_out[c];
+    }
+    a.p  = p.p_in;
+    a.po = p.p_out;
+    return a;
+}
+
+template <typename T>
+int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t st)
+{
+    if (!p.wedge_scratch) return -1;
+    const CouplingArgs<T> a   = coupling_args(p);
+    const int             nc  = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
+    const int             nlc = (p.nl + 1) / 2, nrc = (p.nr + 1) / 2;
+    const int             ncc = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
+    div_cells_kernel<T><<<(nc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
+    div_scatter_kernel<T><<<(ncc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
+    return launch_status(2);
 }
 
 template <typename T>
 int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t st)
 {
-    CouplingArgs<T> a{};
-    a.nl = p.nl;
-    a.nr = p.nr;
-    a.coords = p.coords;
-    a.radii  = p.radii;
-    a.bc_cmb = p.bc_cmb;
-    a.bc_surf = p.bc_surf;
-    a.p      = p.p_in;
-    for (int c = 0; c < 3; ++c) a.uo[c] = p.u_out[c];
-    const int thr = p.nr - 1 >= 64 ? 64 : 32;
-    gradient_kernel<T><<<cell_grid(p.nl, p.nr, thr), thr, 0, st>>>(a);
+    if (!p.wedge_scratch) return -1;
+    const CouplingArgs<T> a  = coupling_args(p);
+    const int             nc = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
+    const int64_t         n  = 10ll * p.nl * p.nl * p.nr;
+    grad_cells_kernel<T><<<(nc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
+    grad_gather_kernel<T><<<static_cast<int>((n + 127) / 128), 128, 0, st>>>(a, p.wedge_scratch, p.add);
+    return launch_status(2);
+}
+
+template <typename T>
+int column_geometry_table(int nl, const T* coords, T* out, cudaStream_t st)
+{
+    const int n = 10 * (nl - 1) * (nl - 1);
+    colgeo_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(nl, coords, out);
     return launch_status();
 }
 
@@ -352,6 +490,7 @@ int vector_mass_add(int nl, int nr, const T* coords, const T* radii, const T* co
 #define TN_INST(T)                                                                                                 \
     template int divergence_apply<T>(const CouplingLaunch<T>&, cudaStream_t);                                     \
     template int gradient_apply<T>(const CouplingLaunch<T>&, cudaStream_t);                                       \
+    template int column_geometry_table<T>(int, const T*, T*, cudaStream_t);                                       \
     template int kmass_lumped_add<T>(int, int, const T*, const T*, const T*, T*, cudaStream_t);                  \
     template int vector_mass_add<T>(int, int, const T*, const T*, const T* const*, T* const*, cudaStream_t);
 TN_INST(double)

@@ -58,15 +58,24 @@ template <typename T>
 struct CouplingLaunch {
     int      nl = 0, nr = 0;  // fine (velocity) level
     const T* coords = nullptr;
+    const T* colgeo = nullptr;  // per-column wedge geometry (column_geometry_table)
     const T* radii  = nullptr;
+    int      add    = 0;        // gradient: 1 accumulates into u_out, 0 overwrites
+    T*       wedge_scratch = nullptr;  // 2 values per fine cell
     int      bc_cmb = 1, bc_surf = 1;
     const T* u[3]     = {nullptr, nullptr, nullptr};  // divergence input
     T*       p_out    = nullptr;                      // divergence output (coarse)
     const T* p_in     = nullptr;                      // gradient input (coarse)
     T*       u_out[3] = {nullptr, nullptr, nullptr};  // gradient output
 };
+// divergence accumulates into p_out (callers zero it for Replace); the
+// gradient writes (or with add accumulates into) every node of u_out.
 template <typename T>
 int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t stream);
+// e1, e2, e3 (columns of M^-T) and |det M| of both wedges of every lateral
+// column, (10, nl-1, nl-1, 20)
+template <typename T>
+int column_geometry_table(int nl, const T* coords, T* out, cudaStream_t stream);
 template <typename T>
 int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t stream);
 template <typename T>
@@ -230,6 +239,8 @@ template <typename T>
 int flag_nonfinite(int64_t n, const T* a, int* flag_dev, cudaStream_t st);
 int widen_check(int64_t n, const float* in, double* out, int* flag_dev, cudaStream_t st);
 int coarse_pcg(const CoarsePcgArgs& args, cudaStream_t st);
+// decide and cache the launch configuration for a level (call outside graph capture)
+int coarse_pcg_prepare(int nl, int nr);
 int coarse_pcg_partials_size();
 int coarse_pcg_cluster_size();
 

@@ -105,6 +105,7 @@ DevBuf upload(const std::vector<T>& v)
 struct DeviceLevel {
     ShellLevel host;
     DevBuf     coords64, coords32;  // (10, nl, nl, 3)
+    DevBuf     colgeo64, colgeo32;  // (10, nl-1, nl-1, 20) per-column wedge geometry
     DevBuf     radii64, radii32;    // (nr)
     DevBuf     owned_lat;           // (10, nl, nl) uint8
     DevBuf     dup_offset, dup_members;
@@ -119,6 +120,8 @@ struct DeviceLevel {
     const T* coords() const;
     template <typename T>
     const T* radii() const;
+    template <typename T>
+    const T* colgeo() const;
 };
 template <>
 inline const double* DeviceLevel::coords<double>() const
@@ -129,6 +132,16 @@ template <>
 inline const float* DeviceLevel::coords<float>() const
 {
     return coords32.as<float>();
+}
+template <>
+inline const double* DeviceLevel::colgeo<double>() const
+{
+    return colgeo64.as<double>();
+}
+template <>
+inline const float* DeviceLevel::colgeo<float>() const
+{
+    return colgeo32.as<float>();
 }
 template <>
 inline const double* DeviceLevel::radii<double>() const
@@ -213,6 +226,7 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st);
 
 // B (DivergenceKerngen): velocity level -> pressure level (level - 1).
 struct DivergenceOp : Operator {
+    mutable DevBuf scratch;  // one value per fine wedge
     int  src_components() const override { return 3; }
     int  dst_components() const override { return 1; }
     bool dst_on_coarse() const override { return true; }
@@ -223,6 +237,7 @@ struct DivergenceOp : Operator {
 
 // B^T (GradientKerngen): pressure level -> velocity level.
 struct GradientOp : Operator {
+    mutable DevBuf scratch;  // one value per fine wedge
     int  src_components() const override { return 1; }
     int  dst_components() const override { return 3; }
     void apply(void* const* src, void* const* dst, cudaStream_t st) override;

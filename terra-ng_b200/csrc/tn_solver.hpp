@@ -112,6 +112,7 @@ struct StokesOptions {
     double    rtol = 1e-8, atol = 1e-12;
     bool      normalize_pressure = true;
     bool      project_pressure_mean = false;  // treat constant pressure as a null vector (see solve())
+    bool      use_graphs = true;              // replay each Arnoldi step as a captured CUDA graph
     MgOptions mg;
 };
 
@@ -126,6 +127,9 @@ class StokesSolver {
     // taken from eta at the pressure nodes).
     StokesSolver(const Shell* sh, int vlevel, const double* eta_nodal, const double* eta_cell, const double* k_schur,
                  int bc_cmb, int bc_surf, const StokesOptions& o, cudaStream_t st);
+    ~StokesSolver();
+    StokesSolver(const StokesSolver&)            = delete;
+    StokesSolver& operator=(const StokesSolver&) = delete;
     // u, p in/out (initial guess, solution); f_u, f_p right-hand side; caller's
     // component arrays. Synchronous. Returns true when the tolerance was met.
     bool solve(double* const* u, double* p, const double* const* fu, const double* fp, cudaStream_t st);
@@ -148,7 +152,12 @@ class StokesSolver {
     const StokesOptions& options() const { return opt_; }
 
   private:
+    static constexpr int kH0   = 2;                      // Hessenberg column in scalar slots kH0..
+    static constexpr int kProj = Scratch::kScalars - 1;  // scalar slot of the pressure-mean projection
     bool solve_internal(cudaStream_t st);  // x_ (initial guess -> solution), b_
+    void step_body(int j, cudaStream_t st);
+    void arnoldi_tail(int j, cudaStream_t st);
+    void run_step(int j, cudaStream_t st);
     void precondition(const DVec<double>& v, DVec<double>& z, cudaStream_t st);
     void stokes_apply(const DVec<double>& x, DVec<double>& y, cudaStream_t st);
     void copy_in(DVec<double>& v, const double* const* u, const double* p, cudaStream_t st);
@@ -169,6 +178,9 @@ class StokesSolver {
     DVec<double>                       x_, b_, r_, w_, t_;
     std::vector<DVec<double>>          V_, Z_;
     DVec<float>                        t32_, z32_;
+    std::vector<cudaGraphExec_t>       graphs_;
+    std::vector<int>                   graph_kernels_;  // kernels captured in each graph
+    cudaStream_t                       ws_ = nullptr;
 };
 
 struct VelocitySolverOptions {

@@ -47,6 +47,7 @@ class SolverOptions(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("normalize_pressure", ctypes.c_int),
         ("project_pressure_mean", ctypes.c_int),
+        ("cuda_graphs", ctypes.c_int),
     ]
 
 

@@ -141,6 +141,19 @@ int tn_operator_apply(tn_operator* op, const void* const* src_dev, void* const* 
 int tn_epsdivdiv_vjp(tn_operator* op, const void* const* u_dev, const void* const* lambda_dev,
                      void* grad_logeta_cell_dev, void* const* grad_u_dev, void* stream);
 
+/* Divergence B of velocity_level -> velocity_level-1 in Replace +
+ * CommunicateAdditively mode (the same kernels and result as a
+ * tn_divergence_create operator's tn_operator_apply) that allocates nothing:
+ * its per-wedge scratch is a fixed 8 MiB static device array, enough for
+ * velocity levels up to 5 (larger levels return TN_ERR_ARG). No counterpart in
+ * the reference. For callers that cannot allocate device memory when they
+ * apply the operator. Calls that overlap in time share the scratch and race;
+ * the first call on a device does the set-up (looks up the scratch address)
+ * and should come before any stream capture. u_dev: 3 velocity components,
+ * p_dev: pressure. */
+int tn_divergence_apply_noalloc(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
+                                const void* const* u_dev, void* p_dev, void* stream);
+
 /* Lumped k-weighted pressure mass diagonal, 6-point rule, interface-summed
  * (KMass with set_lumped_diagonal, src/terra/fe/wedge/operators/shell/
  * kmass.hpp:98-181; used with k = 1/eta as the Schur preconditioner,

@@ -861,3 +861,10 @@ int tn_solver_level_matrices(tn_solver* s, int level, double* mats_host)
 }
 
 }  // extern "C"
+
+// Shell of an opaque handle and the thread's last-error message, for entry
+// points defined in other translation units.
+namespace tn {
+Shell* shell_of(tn_shell* s) { return s ? s->impl.get() : nullptr; }
+void   set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace tn

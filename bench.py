@@ -66,8 +66,11 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64"],
-                    help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator apply")
+    ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "adjoint-L5",
+                                                             "solve-L7"],
+                    help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
+                         "apply; adjoint-L5: the L5 misfit gradient with a finite-difference check; solve-L7: "
+                         "the L7 mixed and FP64 solves plus one adjoint gradient")
     return ap.parse_args()
 
 
@@ -230,11 +233,14 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
-def _time_apply(T, torch, shell, eta, dtype, steps, flush):
+def _time_apply(T, torch, shell, eta, dtype, steps, flush, level=None, eta_cell=None):
     """Average device time of the standalone fine-level apply (kernel + interface sum)."""
-    level = NUM_LEVELS - 1
+    level = NUM_LEVELS - 1 if level is None else level
     nl, nr = shell.dims(level)
-    op = T.EpsDivDiv(shell, level, k=eta.to(dtype), bc_cmb=BCS[0], bc_surface=BCS[1])
+    if eta_cell is not None:
+        op = T.EpsDivDiv(shell, level, k_cell=eta_cell.to(dtype), bc_cmb=BCS[0], bc_surface=BCS[1])
+    else:
+        op = T.EpsDivDiv(shell, level, k=eta.to(dtype), bc_cmb=BCS[0], bc_surface=BCS[1])
     src = T.random_vector(shell, level, 3, 77, dtype=dtype)
     dst = torch.zeros_like(src)
     for _ in range(3):
@@ -431,12 +437,246 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
+def _stokes_vectors(torch, shell, level, dev):
+    nl, nr = shell.dims(level)
+    nlp, nrp = shell.dims(level - 1)
+    x = [torch.zeros((10, nl, nl, nr), dtype=torch.float64, device=dev) for _ in range(3)]
+    x.append(torch.zeros((10, nlp, nlp, nrp), dtype=torch.float64, device=dev))
+    return x
+
+
+def _timed(torch, fn):
+    """Device seconds of fn() on the current stream (synchronised on both sides)."""
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def run_adjoint_l5(a):
+    """Misfit gradient at level 5 (10 x 33 x 33 x 33 velocity nodes, hierarchy L2..L5) with per-cell
+    viscosity: log-uniform [1, 1e4] lateral blocks in a smooth background. J = 1/2 ||u - u_obs||^2 over
+    owned nodes, u_obs from a seeded perturbation of log-viscosity. One forward solve, one adjoint solve and
+    the backward kernel are timed (mixed precision, rtol 1e-8). The gradient (forward and adjoint to 1e-14)
+    is checked against central differences along 32 seeded element directions at step 1e-6 (and the first 8
+    at step 1e-5), each perturbed forward solve warm-started from the unperturbed solution and stopped at an
+    absolute residual of 1e-14 ||b||, and against the gradient of the FP64 solver."""
+    import numpy as np
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    level, nlev, bcs = 5, 4, BCS
+    dev = torch.device("cuda", 0)
+    g = T.Shell(level, num_levels=nlev)
+    fine = nlev - 1
+    eta = S.cell_viscosity_blocks(g, fine, seed=3, tiles=4, fraction=0.3, max_log10=4.0,
+                                  background_log_amplitude=0.5 * math.log(10.0))
+    theta = np.log(eta)
+    ks = torch.tensor(S.schur_coefficient_from_cells(g, fine, eta), device=dev)
+    f = S.buoyancy_rhs(g, fine, S.temperature(g, fine, seed=SEED_TEMP), *bcs)
+    rng = np.random.default_rng(5)
+    theta_obs = theta + 0.1 * rng.standard_normal(theta.shape)
+    own = torch.tensor(g.ownership(fine), device=dev).bool()
+
+    def solver(th, rtol, atol=0.0, mixed=1):
+        return T.StokesSolver(g, eta_cell=torch.tensor(np.exp(th), device=dev), k_schur=ks, bc_cmb=bcs[0],
+                              bc_surface=bcs[1], relative_tolerance=rtol, absolute_tolerance=atol,
+                              max_iterations=20000, project_pressure_mean=1, normalize_pressure=0,
+                              mixed_precision=mixed)
+
+    def forward(s, x0=None):
+        x = _stokes_vectors(torch, g, fine, dev)
+        if x0 is not None:
+            for t, t0 in zip(x, x0):
+                t.copy_(t0)
+        rhs = [f[c].contiguous() for c in range(3)] + [torch.zeros_like(x[3])]
+        ok = s.solve(x, rhs)
+        return x, ok
+
+    bnorm = math.sqrt(g.dot([f[c] for c in range(3)], [f[c] for c in range(3)], level=fine))
+    s_obs = solver(theta_obs, 1e-14)
+    x_obs, _ = forward(s_obs)
+    u_obs = [x_obs[c] for c in range(3)]
+    del s_obs
+
+    # timed gradient at the production tolerance
+    s8 = solver(theta, 1e-8)
+    grad8 = torch.zeros(theta.shape, dtype=torch.float64, device=dev)
+    for _ in range(max(1, a.warmup)):
+        x8, _ = forward(s8)
+        s8.misfit_gradient(x8, u_obs, grad8)
+    steps = max(1, a.steps)
+    t_fwd = t_adj = 0.0
+    for _ in range(steps):
+        dt, (x8, ok) = _timed(torch, lambda: forward(s8))
+        t_fwd += dt / steps
+        dt, _ = _timed(torch, lambda: s8.misfit_gradient(x8, u_obs, grad8))
+        t_adj += dt / steps
+    its_fwd = s8.result()[0]
+    del s8
+
+    # gradient at 1e-14 (mixed and FP64) and the finite-difference check
+    grads, its14 = {}, {}
+    x_base = None
+    for name, mixed in (("mixed", 1), ("fp64", 0)):
+        s = solver(theta, 1e-14, mixed=mixed)
+        x, _ = forward(s)
+        its14[name] = s.result()[0]
+        if mixed:
+            x_base = [t.clone() for t in x]
+        gr = torch.zeros(theta.shape, dtype=torch.float64, device=dev)
+        s.misfit_gradient(x, u_obs, gr)
+        grads[name] = gr.cpu().numpy()
+        del s
+    gm, gd = grads["mixed"], grads["fp64"]
+    mixed_vs_fp64 = float(np.linalg.norm(gm - gd) / np.linalg.norm(gd))
+
+    fd_its = []
+
+    def J(th):
+        s = solver(th, 0.0, atol=1e-14 * bnorm)
+        x, _ = forward(s, x_base)
+        fd_its.append(s.result()[0])
+        return 0.5 * float(sum(((x[c] - u_obs[c])[own] ** 2).sum() for c in range(3)))
+
+    drng = np.random.default_rng(6)
+    dirs = [drng.standard_normal(theta.shape) for _ in range(32)]
+    fd_err = {}
+    t0 = time.perf_counter()
+    for h, nd in ((1e-6, 32), (1e-5, 8)):
+        errs = []
+        for d in dirs[:nd]:
+            fd = (J(theta + h * d) - J(theta - h * d)) / (2 * h)
+            ad = float(np.sum(gd * d))
+            errs.append(abs(fd - ad) / abs(ad))
+        fd_err[f"{h:g}"] = {"directions": nd, "max": max(errs), "median": float(np.median(errs))}
+    t_fd = time.perf_counter() - t0
+    line = {"metric": "L5 adjoint log-viscosity gradient time (forward + adjoint solve + VJP, rtol 1e-8)",
+            "value": t_fwd + t_adj, "unit": "s/gradient", "n_gpus": 1, "steps": steps, "warmup": a.warmup,
+            "ms_per_step": (t_fwd + t_adj) * 1e3, "higher_is_better": False, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "L5 adjoint gradient (10x33x33x33 velocity nodes, hierarchy L2..L5), no-slip / "
+                                   "free-slip, per-cell viscosity: log-uniform [1, 1e4] 8x8-cell lateral blocks in "
+                                   "a smooth SH background (factor 10), J = 1/2||u - u_obs||^2, u_obs from log-eta "
+                                   "+ 0.1 N(0,1)", "viscosity_contrast": float(eta.max() / eta.min())},
+            "forward_s": t_fwd, "adjoint_and_vjp_s": t_adj, "forward_iterations_1e-8": its_fwd,
+            "forward_iterations_1e-14": its14,
+            "fd_check": {"rel_err_by_step": fd_err, "base_solve_rtol": 1e-14,
+                         "perturbed_solve_atol_over_bnorm": 1e-14, "warm_start": True,
+                         "iterations_per_perturbed_solve": {"min": min(fd_its), "max": max(fd_its)},
+                         "seconds": t_fd},
+            "gradient_mixed_vs_fp64_rel_l2": mixed_vs_fp64}
+    print(json.dumps(line), flush=True)
+
+
+def run_solve_l7(a):
+    """Level 7: 10 x 129 x 129 x 129 velocity nodes (64M velocity dofs), pressure on L6, hierarchy L2..L7,
+    per-cell viscosity with contrast 1e3 including a x30 jump below r = 0.9, seeded buoyancy right-hand side.
+    Times the mixed and the FP64 solve to 1e-8 and one adjoint gradient with the mixed solver."""
+    import gc
+
+    import numpy as np
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    level, nlev, bcs = 7, 6, BCS
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = T.Shell(level, num_levels=nlev)
+    fine = nlev - 1
+    t0 = time.perf_counter()
+    eta = S.cell_viscosity_radial_jump(g, fine, seed=SEED_ETA, contrast=1e3, jump=30.0, r_jump=0.9)
+    ks = torch.tensor(S.schur_coefficient_from_cells(g, fine, eta), device=dev)
+    eta_d = torch.tensor(eta, device=dev)
+    f = S.buoyancy_rhs(g, fine, S.temperature(g, fine, seed=SEED_TEMP), *bcs)
+    t_inputs = time.perf_counter() - t0
+    opts = dict(k_schur=ks, bc_cmb=bcs[0], bc_surface=bcs[1], relative_tolerance=1e-8, absolute_tolerance=0.0,
+                max_iterations=5000, restart=30, project_pressure_mean=1, normalize_pressure=0)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+
+    # observations from a perturbed viscosity (one mixed solve, solver released before the timed ones)
+    rng = np.random.default_rng(7)
+    s_obs = T.StokesSolver(g, eta_cell=torch.tensor(eta * np.exp(0.1 * rng.standard_normal(eta.shape)),
+                                                    device=dev), mixed_precision=1, **opts)
+    x_obs = _stokes_vectors(torch, g, fine, dev)
+    b = [f[c].contiguous() for c in range(3)] + [torch.zeros_like(x_obs[3])]
+    s_obs.solve(x_obs, b)
+    u_obs = [x_obs[c] for c in range(3)]
+    del s_obs
+    gc.collect()
+
+    res, setup = {}, {}
+    steps = max(1, a.steps)
+    for name, mixed in (("mixed", 1), ("fp64", 0)):
+        dt, s = _timed(torch, lambda: T.StokesSolver(g, eta_cell=eta_d, mixed_precision=mixed, **opts))
+        setup[name] = dt
+        used = free0 - torch.cuda.mem_get_info(dev)[0]
+        x = _stokes_vectors(torch, g, fine, dev)
+        for _ in range(max(1, a.warmup)):
+            for t in x:
+                t.zero_()
+            s.solve(x, b)
+        ts = []
+        for _ in range(steps):
+            for t in x:
+                t.zero_()
+            dt, _ = _timed(torch, lambda: s.solve(x, b))
+            ts.append(dt)
+        its, rr, conv = s.result()
+        r = {"s": sum(ts) / steps, "iterations": its, "relres": rr, "converged": conv,
+             "device_bytes_with_solver": used}
+        if mixed:
+            grad = torch.zeros(eta.shape, dtype=torch.float64, device=dev)
+            dt, ok = _timed(torch, lambda: s.misfit_gradient(x, u_obs, grad))
+            r["adjoint_gradient_s"] = dt
+            r["adjoint_converged"] = ok
+            r["gradient_finite"] = bool(torch.isfinite(grad).all())
+        res[name] = r
+        del s, x
+        gc.collect()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    peak, peak_kind = _peaks()
+    nl, nr = g.dims(fine)
+    nodes = 10 * nl * nl * nr
+    apply = {}
+    for prec, dt in (("f32", torch.float32), ("f64", torch.float64)):
+        t, _ = _time_apply(T, torch, g, None, dt, 10, flush, level=fine, eta_cell=eta_d)
+        ach = BYTES_PER_NODE[prec] * nodes / t / 1e9
+        apply[prec] = {"ms": t * 1e3, "achieved_gbs": ach, "frac": ach / peak}
+    line = {"metric": "L7 Stokes solve time to 1e-8 (FP32-MG vs FP64)", "value": res["mixed"]["s"],
+            "unit": "s/solve", "n_gpus": 1, "steps": steps, "warmup": a.warmup,
+            "ms_per_step": res["mixed"]["s"] * 1e3, "higher_is_better": False, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "L7 Stokes solve (10x129x129x129 velocity nodes, pressure on L6, hierarchy "
+                                   "L2..L7), no-slip / free-slip, per-cell viscosity contrast 1e3 with a x30 jump "
+                                   "below r = 0.9, seeded buoyancy RHS, FGMRES(30) + block-triangular GMG "
+                                   "preconditioner, rtol 1e-8", "viscosity_contrast": float(eta.max() / eta.min())},
+            "fp64_solve_s": res["fp64"]["s"], "speedup_mixed_vs_fp64": res["fp64"]["s"] / res["mixed"]["s"],
+            "solves": res, "setup_s": setup, "inputs_s": t_inputs,
+            "apply_roofline": {"peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                               "bytes_per_node": BYTES_PER_NODE, **apply}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
-    elif a.workload != "solve":
+    elif a.workload.startswith("apply"):
         run_apply(a)
+    elif a.workload == "adjoint-L5":
+        run_adjoint_l5(a)
+    elif a.workload == "solve-L7":
+        run_solve_l7(a)
     else:
         run_ours(a)
 

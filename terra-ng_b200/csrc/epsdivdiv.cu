@@ -36,6 +36,7 @@
 #include "tn_wedge_math.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace tn {
 namespace {
@@ -52,6 +53,105 @@ template <>
 struct MaxWarps<float> {
     static constexpr int value = 12;
 };
+
+// ---------------------------------------------------------------------------
+// FP32 interior cells two at a time. A lane's radial cells c and c + 32 share
+// their lateral geometry, so the arithmetic of hex_interior runs on float2
+// pairs with the packed FP32 instructions of sm_100 (FFMA2 / FADD2 / FMUL2):
+// one instruction per two cells. Subtraction is fma(b, -1, a), which rounds
+// like a - b. The nodal outputs are assembled per corner: corners 0 and 3
+// belong to one wedge each, corners 1 and 2 to both, with the lateral part
+// lat and radial part rad giving bottom = lat - rad and top = lat + rad.
+// ---------------------------------------------------------------------------
+using f2 = float2;
+__device__ __forceinline__ f2 p_add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 p_sub(f2 a, f2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ f2 p_mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 p_fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 p_bc(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ void hex_interior_x2(const f2 (&u)[4][2][3], const f2 (&ks)[4], f2 kcell, bool q0,
+                                                const float* geo, f2 alpha, f2 beta, f2 dfac, f2 (&out)[4][2][3])
+{
+    f2 S[4][3], Dq[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            S[q][c]  = p_add(u[q][0][c], u[q][1][c]);
+            Dq[q][c] = p_sub(u[q][1][c], u[q][0][c]);
+        }
+    f2 v1w[2][3], v2w[2][3], wvw[2][3];
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const float* gw  = geo + 10 * w;
+        const int    q0i = wedge_corner(w, 0), q1i = wedge_corner(w, 1), q2i = wedge_corner(w, 2);
+        const f2     kv  = q0 ? kcell : p_add(p_add(ks[q0i], ks[q1i]), ks[q2i]);
+        const f2     kw  = p_mul(kv, p_mul(dfac, p_bc(gw[9])));
+        f2           E1[3], E2[3], E3[3], a[3], b[3], D[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            E1[i] = p_mul(alpha, p_bc(gw[i]));
+            E2[i] = p_mul(alpha, p_bc(gw[3 + i]));
+            E3[i] = p_mul(beta, p_bc(gw[6 + i]));
+            a[i]  = p_sub(S[q1i][i], S[q0i][i]);
+            b[i]  = p_sub(S[q2i][i], S[q0i][i]);
+            D[i]  = p_add(p_add(Dq[q0i][i], Dq[q1i][i]), Dq[q2i][i]);
+        }
+        f2 gd[3], h[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) gd[i] = p_fma(E3[i], D[i], p_fma(E2[i], b[i], p_mul(E1[i], a[i])));
+        // h[k] for the pair (i, j) = (0,1), (0,2), (1,2)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int i = k == 2 ? 1 : 0, j = k == 0 ? 1 : 2;
+            f2        t = p_mul(E1[i], a[j]);
+            t           = p_fma(E1[j], a[i], t);
+            t           = p_fma(E2[i], b[j], t);
+            t           = p_fma(E2[j], b[i], t);
+            t           = p_fma(E3[i], D[j], t);
+            h[k]        = p_fma(E3[j], D[i], t);
+        }
+        const f2 tr  = p_add(p_add(gd[0], gd[1]), gd[2]);
+        const f2 nkd = p_mul(kw, p_mul(p_bc(-2.0f / 3.0f), tr));
+        const f2 k2  = p_add(kw, kw);
+        const f2 s00 = p_fma(k2, gd[0], nkd), s11 = p_fma(k2, gd[1], nkd), s22 = p_fma(k2, gd[2], nkd);
+        const f2 s01 = p_mul(kw, h[0]), s02 = p_mul(kw, h[1]), s12 = p_mul(kw, h[2]);
+        // sigma E for E = E1, E2, E3 (sigma symmetric)
+        auto sig = [&](const f2 (&E)[3], f2 (&o)[3]) {
+            o[0] = p_fma(s02, E[2], p_fma(s01, E[1], p_mul(s00, E[0])));
+            o[1] = p_fma(s12, E[2], p_fma(s11, E[1], p_mul(s01, E[0])));
+            o[2] = p_fma(s22, E[2], p_fma(s12, E[1], p_mul(s02, E[0])));
+        };
+        sig(E1, v1w[w]);
+        sig(E2, v2w[w]);
+        sig(E3, wvw[w]);
+    }
+    // corner 0: wedge 0 m=0; corner 3: wedge 1 m=0; corner 1: w0 m=1 + w1 m=2;
+    // corner 2: w0 m=2 + w1 m=1 (wedge_corner(1, m) = 3 - m)
+    const f2 m1 = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const f2 v120 = p_add(v1w[0][c], v2w[0][c]);
+        const f2 v121 = p_add(v1w[1][c], v2w[1][c]);
+        const f2 rad  = p_add(wvw[0][c], wvw[1][c]);
+        const f2 lat1 = p_add(v1w[0][c], v2w[1][c]);
+        const f2 lat2 = p_add(v2w[0][c], v1w[1][c]);
+        out[0][0][c]  = p_mul(p_add(v120, wvw[0][c]), m1);
+        out[0][1][c]  = p_sub(wvw[0][c], v120);
+        out[3][0][c]  = p_mul(p_add(v121, wvw[1][c]), m1);
+        out[3][1][c]  = p_sub(wvw[1][c], v121);
+        out[1][0][c]  = p_sub(lat1, rad);
+        out[1][1][c]  = p_add(lat1, rad);
+        out[2][0][c]  = p_sub(lat2, rad);
+        out[2][1][c]  = p_add(lat2, rad);
+    }
+}
+
+// Packed FP32 pairs for the interior arithmetic: FP32, an even number of
+// radial cells per lane, apply mode (the diagonal mode stays scalar).
+template <typename T, int CPL, bool DIAG>
+inline constexpr bool kPackedPairs = std::is_same<T, float>::value && (CPL % 2 == 0) && !DIAG;
 
 template <typename T>
 struct EddArgs {
@@ -271,36 +371,52 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
             }
         };
 
+        // Staged inputs of cell rc of this column (the caller checks validity).
+        auto load_cell = [&](int rc, T (&u)[4][2][3], T (&ks)[4], T& kcell) {
+            const int e0 = (yc - ylo) * nr + rc;      // corners dy = 0
+            const int e1 = (yc + 1 - ylo) * nr + rc;  // corners dy = 1
 #pragma unroll
-        for (int j = 0; j < CPL; ++j) {
-            const int rc = lane + 32 * j;
-            T         out[4][2][3];
-            if (ok && cell_col_ok && rc < nr - 1) {
-                const int e0 = (yc - ylo) * nr + rc;       // corners dy = 0
-                const int e1 = (yc + 1 - ylo) * nr + rc;   // corners dy = 1
-                T         u[4][2][3], ks[4];
+            for (int q = 0; q < 4; ++q) {
+                const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
+                const int*           off = (q & 1) ? offB : offA;
+                const int            e   = (q >> 1) ? e1 : e0;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
-                    const int*           off = (q & 1) ? offB : offA;
-                    const int            e   = (q >> 1) ? e1 : e0;
-                    T                    kb, kt;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap) + off[c];
-                        u[q][0][c]  = fr[e];
-                        u[q][1][c]  = fr[e + 1];
-                    }
-                    if (!q0) {
-                        const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap) + off[3];
-                        kb          = kr[e];
-                        kt          = kr[e + 1];
-                        ks[q]       = kb + kt;
-                    } else {
-                        ks[q] = T(0);
-                    }
+                for (int c = 0; c < 3; ++c) {
+                    const T* fr = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap) + off[c];
+                    u[q][0][c]  = fr[e];
+                    u[q][1][c]  = fr[e + 1];
                 }
-                const T kcell = q0 ? A.kq0[node_index(nl - 1, nr - 1, d, x, yc, rc)] : T(0);
+                if (!q0) {
+                    const T* kr = reinterpret_cast<const T*>(row + static_cast<size_t>(3) * L.rowcap) + off[3];
+                    ks[q]       = kr[e] + kr[e + 1];
+                } else {
+                    ks[q] = T(0);
+                }
+            }
+            kcell = q0 ? A.kq0[node_index(nl - 1, nr - 1, d, x, yc, rc)] : T(0);
+        };
+        // Unmodified side-s values of cell rc (boundary rows).
+        auto load_raw = [&](int rc, int side, T (&raw)[4][3]) {
+            const int e0 = (yc - ylo) * nr + rc + side;
+            const int e1 = (yc + 1 - ylo) * nr + rc + side;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
+                const int*           off = (q & 1) ? offB : offA;
+                const int            e   = (q >> 1) ? e1 : e0;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    raw[q][c] = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap)[off[c] + e];
+            }
+        };
+        const T* bco_col = bcof + (static_cast<size_t>(w) * (cx + 1) + i) * 2 * 18;
+
+        // Scalar path: one cell (all modes).
+        auto scalar_cell = [&](int j, T (&out)[4][2][3]) {
+            const int rc = lane + 32 * j;
+            if (ok && cell_col_ok && rc < nr - 1) {
+                T u[4][2][3], ks[4], kcell;
+                load_cell(rc, u, ks, kcell);
                 if (DIAG) {
                     const int bcs[2] = {cbc[j][0], cbc[j][1]};
                     T         nrm[4][3];
@@ -325,18 +441,9 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
                     for (int side = 0; side < 2; ++side) {
                         if (!(side == 0 ? b0 : b1)) continue;
                         T raw[4][3];
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const unsigned char* row = reinterpret_cast<const unsigned char*>((q & 1) ? rowB : rowA);
-                            const int*           off = (q & 1) ? offB : offA;
-                            const int            e   = ((q >> 1) ? e1 : e0) + side;
-#pragma unroll
-                            for (int c = 0; c < 3; ++c)
-                                raw[q][c] = reinterpret_cast<const T*>(row + static_cast<size_t>(c) * L.rowcap)[off[c] + e];
-                        }
+                        load_raw(rc, side, raw);
                         side_outputs<T>(out, side, side == 0 ? cbc[j][0] : cbc[j][1], ks, kcell, q0,
-                                        bcof + ((static_cast<size_t>(w) * (cx + 1) + i) * 2 + side) * 18, nrm_col, raw,
-                                        side == 0 ? un0 : un1);
+                                        bco_col + side * 18, nrm_col, raw, side == 0 ? un0 : un1);
                     }
                 }
             } else {
@@ -347,25 +454,107 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 #pragma unroll
                         for (int c = 0; c < 3; ++c) out[q][sd][c] = T(0);
             }
-            {
-                T nv[4][3], top[4][3];
+        };
+
+        // Radial sums of cell j's outputs into node values.
+        auto combine = [&](int j, const T (&out)[4][2][3]) {
+            T nv[4][3], top[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    top[q][c]     = out[q][1][c];
+                    const T up    = shfl_up(top[q][c], 1);
+                    const T below = lane > 0 ? up : (j > 0 ? carry31[q][c] : T(0));
+                    nv[q][c]      = out[q][0][c] + below;
+                }
+            finish_node(j, nv);
+            if (j == j_top) finish_node(CPL, top);
+            if (j + 1 < CPL) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        top[q][c]      = out[q][1][c];
-                        const T up     = shfl_up(top[q][c], 1);
-                        const T below  = lane > 0 ? up : (j > 0 ? carry31[q][c] : T(0));
-                        nv[q][c]       = out[q][0][c] + below;
-                    }
-                finish_node(j, nv);
-                if (j == j_top) finish_node(CPL, top);
-                if (j + 1 < CPL) {
+                    for (int c = 0; c < 3; ++c) carry31[q][c] = __shfl_sync(0xffffffffu, top[q][c], 31);
+            }
+        };
+
+        if constexpr (kPackedPairs<T, CPL, DIAG>) {
+            // FP32: cells (j, j + 1) of the lane as one packed pair
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
+            for (int j = 0; j < CPL; j += 2) {
+                const int  rcA = lane + 32 * j, rcB = rcA + 32;
+                const bool vA  = ok && cell_col_ok && rcA < nr - 1;
+                const bool vB  = ok && cell_col_ok && rcB < nr - 1;
+                T          uA[4][2][3], uB[4][2][3], ksA[4], ksB[4], kA = T(0), kB = T(0);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) carry31[q][c] = __shfl_sync(0xffffffffu, top[q][c], 31);
+                for (int q = 0; q < 4; ++q) {
+                    ksA[q] = ksB[q] = T(0);
+#pragma unroll
+                    for (int sd = 0; sd < 2; ++sd)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) uA[q][sd][c] = uB[q][sd][c] = T(0);
                 }
+                if (vA) load_cell(rcA, uA, ksA, kA);
+                if (vB) load_cell(rcB, uB, ksB, kB);
+                // boundary cells: CMB is cell 0 (lane 0, j = 0), the surface cell nr - 2
+                const bool b0A = vA && cbc[j][0] != 0, b1A = vA && cbc[j][1] != 0;
+                const bool b0B = vB && cbc[j + 1][0] != 0, b1B = vB && cbc[j + 1][1] != 0;
+                T          un0A[4], un1A[4], un0B[4], un1B[4];
+                if (b0A) side_inputs<T>(uA, 0, cbc[j][0], nrm_col, un0A);
+                if (b1A) side_inputs<T>(uA, 1, cbc[j][1], nrm_col, un1A);
+                if (b0B) side_inputs<T>(uB, 0, cbc[j + 1][0], nrm_col, un0B);
+                if (b1B) side_inputs<T>(uB, 1, cbc[j + 1][1], nrm_col, un1B);
+                f2 u2[4][2][3], ks2[4], o2[4][2][3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    ks2[q] = make_float2(ksA[q], ksB[q]);
+#pragma unroll
+                    for (int sd = 0; sd < 2; ++sd)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) u2[q][sd][c] = make_float2(uA[q][sd][c], uB[q][sd][c]);
+                }
+                hex_interior_x2(u2, ks2, make_float2(kA, kB), q0, reinterpret_cast<const float*>(g),
+                                make_float2(alpha[j], alpha[j + 1]), make_float2(beta[j], beta[j + 1]),
+                                make_float2(dfac[j], dfac[j + 1]), o2);
+                T oA[4][2][3], oB[4][2][3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int sd = 0; sd < 2; ++sd)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            oA[q][sd][c] = o2[q][sd][c].x;
+                            oB[q][sd][c] = o2[q][sd][c].y;
+                        }
+                if (b0A || b1A) {
+#pragma unroll
+                    for (int side = 0; side < 2; ++side) {
+                        if (!(side == 0 ? b0A : b1A)) continue;
+                        T raw[4][3];
+                        load_raw(rcA, side, raw);
+                        side_outputs<T>(oA, side, cbc[j][side], ksA, kA, q0, bco_col + side * 18, nrm_col, raw,
+                                        side == 0 ? un0A : un1A);
+                    }
+                }
+                if (b0B || b1B) {
+#pragma unroll
+                    for (int side = 0; side < 2; ++side) {
+                        if (!(side == 0 ? b0B : b1B)) continue;
+                        T raw[4][3];
+                        load_raw(rcB, side, raw);
+                        side_outputs<T>(oB, side, cbc[j + 1][side], ksB, kB, q0, bco_col + side * 18, nrm_col, raw,
+                                        side == 0 ? un0B : un1B);
+                    }
+                }
+                combine(j, oA);
+                combine(j + 1, oB);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                T out[4][2][3];
+                scalar_cell(j, out);
+                combine(j, out);
             }
         }
         __syncthreads();

@@ -73,6 +73,7 @@ void apply(const DeviceLevel& L, const DeviceLevel& Lc, int bc_cmb, int bc_surf,
     c.nr      = L.nr();
     c.coords  = L.coords<T>();
     c.colgeo  = L.colgeo<T>();
+    c.radgeo  = L.radgeo<T>();
     c.radii   = L.radii<T>();
     c.bc_cmb  = bc_cmb;
     c.bc_surf = bc_surf;

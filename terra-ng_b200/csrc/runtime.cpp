@@ -65,6 +65,14 @@ std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, 
                 throw Error(kErrCuda, "column geometry launch failed");
             cuda_check(cudaDeviceSynchronize(), "column geometry");
         }
+        if (h.nr > 1) {
+            dl->radgeo64.alloc(static_cast<size_t>(h.nr - 1) * 3 * sizeof(double));
+            dl->radgeo32.alloc(static_cast<size_t>(h.nr - 1) * 3 * sizeof(float));
+            if (radial_geometry_table<double>(h.nr, dl->radii64.as<double>(), dl->radgeo64.as<double>(), nullptr) != 0 ||
+                radial_geometry_table<float>(h.nr, dl->radii32.as<float>(), dl->radgeo32.as<float>(), nullptr) != 0)
+                throw Error(kErrCuda, "radial geometry launch failed");
+            cuda_check(cudaDeviceSynchronize(), "radial geometry");
+        }
         dl->iface.num_classes = static_cast<int>(h.dup_offset.size()) - 1;
         dl->iface.offset      = dl->dup_offset.as<int32_t>();
         dl->iface.members     = dl->dup_members.as<int32_t>();
@@ -255,6 +263,7 @@ void DivergenceOp::apply_t(const T* const* src, T* p, cudaStream_t st) const
     c.nr     = L.nr();
     c.coords = L.coords<T>();
     c.colgeo = L.colgeo<T>();
+    c.radgeo = L.radgeo<T>();
     c.radii  = L.radii<T>();
     c.bc_cmb = bc_cmb;
     c.bc_surf = bc_surf;
@@ -285,6 +294,7 @@ void GradientOp::apply_t(const T* p, T* const* dst, cudaStream_t st) const
     c.nr      = L.nr();
     c.coords  = L.coords<T>();
     c.colgeo  = L.colgeo<T>();
+    c.radgeo  = L.radgeo<T>();
     c.radii   = L.radii<T>();
     c.add     = apply_mode == 1 ? 1 : 0;
     const size_t need = sizeof(T) * 2 * static_cast<size_t>(L.cells());

@@ -92,6 +92,37 @@ __global__ void __launch_bounds__(kThreads) vdot_kernel(VecDesc L, const T* __re
     block_finish(acc, rs, out, take_sqrt);
 }
 
+// L2 residency of the Gram-Schmidt target. One Arnoldi step reads and writes
+// w once per basis vector; w (the level-6 Stokes vector is 69 MB) fits in the
+// 126 MB L2 while the basis vectors stream past it. w is loaded and stored
+// with an evict_last policy and the basis vectors with streaming loads, so
+// each step costs about one basis-vector read of DRAM traffic instead of two
+// vectors plus w. The last step of an Arnoldi iteration (the norm) stores w
+// with evict_normal, which hands the lines back to ordinary replacement before
+// the preconditioner runs.
+__device__ __forceinline__ uint64_t l2_policy(bool keep)
+{
+    uint64_t p;
+    if (keep)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ double2 ld_policy(const double2* a, uint64_t pol)
+{
+    double2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ void st_policy(double2* a, double2 v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol)
+                 : "memory");
+}
+
 // Gram-Schmidt step over pairs of entries (components start at multiples of
 // 64 entries, so pairs are 16-byte aligned); the odd tail entry is handled
 // by the thread that owns pair index n / 2.
@@ -100,9 +131,10 @@ __global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __rest
                                                         const double* __restrict__ vdot, RedScratch rs, double* out,
                                                         int take_sqrt)
 {
-    const double  h      = vsub ? *hsub : 0.0;
-    double        acc    = 0.0;
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const double   h      = vsub ? *hsub : 0.0;
+    const uint64_t pol    = l2_policy(vdot != nullptr);
+    double         acc    = 0.0;
+    const int64_t  stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int s = 0; s < L.nseg; ++s) {
         const VecSeg  S  = L.seg[s];
         const int64_t np = S.n / 2;
@@ -112,14 +144,14 @@ __global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __rest
             const double2* s2 = vsub ? reinterpret_cast<const double2*>(vsub + o) : nullptr;
             const double2* d2 = vdot ? reinterpret_cast<const double2*>(vdot + o) : nullptr;
             for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < np; k += stride) {
-                double2 wv = w2[k];
+                double2 wv = ld_policy(w2 + k, pol);
                 if (s2) {
-                    const double2 sv = s2[k];
+                    const double2 sv = __ldcs(s2 + k);
                     wv.x             = wv.x - h * sv.x;
                     wv.y             = wv.y - h * sv.y;
-                    w2[k]            = wv;
+                    st_policy(w2 + k, wv, pol);
                 }
-                const double2 dv = d2 ? d2[k] : wv;
+                const double2 dv = d2 ? __ldcs(d2 + k) : wv;
                 if (S.owned[lat_of(2 * k, S.rdiv)]) acc += wv.x * dv.x;
                 if (S.owned[lat_of(2 * k + 1, S.rdiv)]) acc += wv.y * dv.y;
             }
@@ -506,33 +538,38 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_kernel(CoarsePcgArg
 // A p. Dots and vector updates then run on local copies, identically (same
 // data, same order) in every CTA, and need no further communication.
 // ---------------------------------------------------------------------------
-__device__ double block_sum_all(double v, double* red)
+// Block-wide sum returned to every thread. The warp sums go to one of two
+// buffers in turn, so a single barrier suffices: a buffer is written again
+// only two calls later, after every thread has passed the barrier of the call
+// in between (and so has finished reading it).
+__device__ double block_sum_all(double v, double* red, int& parity)
 {
-    v = warp_sum(v);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    v           = warp_sum(v);
+    double* buf = red + (parity & 1) * 32;
+    ++parity;
+    if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
     __syncthreads();
     double s = 0.0;
-    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) s += red[k];
+    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) s += buf[k];
     return s;
 }
 
 __device__ __forceinline__ double owned_dot(const double* a, const double* b, int n, int n3, uint64_t rdiv,
-                                             const uint8_t* owned, double* red)
+                                             const uint8_t* owned, double* red, int& parity)
 {
     double acc = 0.0;
     for (int e = threadIdx.x; e < n3; e += blockDim.x) {
         const int c = e / n, j = e - c * n;
         if (owned[lat_of(j, rdiv)]) acc += a[e] * b[e];
     }
-    return block_sum_all(acc, red);
+    return block_sum_all(acc, red, parity);
 }
 
+// dst = A src (all CTAs end with the same full vector). part must be zero on
+// entry and is zero again on return. xch: blockDim.x doubles of scratch.
 __device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const double* src, double* dst, double* part,
-                           int n, int n3, cg::cluster_group& cluster)
+                           double* xch, int n, int n3, cg::cluster_group& cluster)
 {
-    for (int e = threadIdx.x; e < n3; e += blockDim.x) part[e] = 0.0;
-    __syncthreads();
     const int items = 36 * V.cnt;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int lc   = it % V.cnt;
@@ -550,15 +587,42 @@ __device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const doubl
         atomicAdd(part + ca * n + V.node[(w * 6 + na) * V.cpc + lc], acc);
     }
     cluster.sync();
+    // This CTA sums slice [e0, e1) over all CTAs' partials: thread t reads
+    // element e0 + t % sl from the CTAs k, k + ng, ... (k = t / sl), the ng
+    // group sums are combined in a fixed order, and the same thread layout
+    // writes the result to every CTA's dst.
     const unsigned ncta = cluster.num_blocks(), rank = cluster.block_rank();
-    const int      sl   = (n3 + ncta - 1) / ncta;
-    const int      e0 = rank * sl, e1 = e0 + sl < n3 ? e0 + sl : n3;
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        double v = 0.0;
-        for (unsigned c = 0; c < ncta; ++c) v += cluster.map_shared_rank(part, c)[e];
-        for (unsigned c = 0; c < ncta; ++c) cluster.map_shared_rank(dst, c)[e] = v;
+    const int      sl   = (n3 + static_cast<int>(ncta) - 1) / static_cast<int>(ncta);
+    const int      e0 = static_cast<int>(rank) * sl, e1 = e0 + sl < n3 ? e0 + sl : n3;
+    const int      len = e1 > e0 ? e1 - e0 : 0;
+    if (sl <= static_cast<int>(blockDim.x)) {
+        int ng = static_cast<int>(blockDim.x) / sl;
+        if (ng > static_cast<int>(ncta)) ng = static_cast<int>(ncta);
+        const int t = threadIdx.x, k = t / sl, i = t - k * sl;
+        if (k < ng) {
+            double v = 0.0;
+            if (i < len)
+                for (int c = k; c < static_cast<int>(ncta); c += ng) v += cluster.map_shared_rank(part, c)[e0 + i];
+            xch[t] = v;
+        }
+        __syncthreads();
+        if (t < len) {  // column t: group sums in order k = 0, 1, ...
+            double v = xch[t];
+            for (int g = 1; g < ng; ++g) v += xch[g * sl + t];
+            xch[t] = v;
+        }
+        __syncthreads();
+        if (k < ng && i < len)
+            for (int c = k; c < static_cast<int>(ncta); c += ng) cluster.map_shared_rank(dst, c)[e0 + i] = xch[i];
+    } else {
+        for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            double v = 0.0;
+            for (unsigned c = 0; c < ncta; ++c) v += cluster.map_shared_rank(part, c)[e];
+            for (unsigned c = 0; c < ncta; ++c) cluster.map_shared_rank(dst, c)[e] = v;
+        }
     }
     cluster.sync();
+    for (int e = threadIdx.x; e < n3; e += blockDim.x) part[e] = 0.0;
     const int nr = A.nr, iitems = A.num_classes * nr * 3;
     for (int it = threadIdx.x; it < iitems; it += blockDim.x) {
         const int r    = it % nr;
@@ -577,7 +641,9 @@ __device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const doubl
 __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePcgArgs A)
 {
     extern __shared__ __align__(16) unsigned char pcg_smem[];
-    __shared__ double   red[kPcgThreads / 32];
+    __shared__ double   red[2 * 32];
+    __shared__ double   xch[kPcgThreads];
+    int                 parity = 0;
     cg::cluster_group   cluster = cg::this_cluster();
     const unsigned      rank = cluster.block_rank(), ncta = cluster.num_blocks();
     const int           nl = A.nl, nr = A.nr;
@@ -622,9 +688,10 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
     for (int e = threadIdx.x; e < n3; e += blockDim.x) {
         const int c = e / n, j = e - c * n;
         p_s[e]      = A.x[c * S + j];
+        pt_s[e]     = 0.0;
     }
     __syncthreads();
-    rep_matvec(A, V, p_s, ap_s, pt_s, n, n3, cluster);
+    rep_matvec(A, V, p_s, ap_s, pt_s, xch, n, n3, cluster);
     for (int e = threadIdx.x; e < n3; e += blockDim.x) {
         const int    c = e / n, j = e - c * n;
         const double rv = A.b[c * S + j] - ap_s[e];
@@ -632,15 +699,15 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
         p_s[e]          = rv;
     }
     __syncthreads();
-    double       rr   = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red);
+    double       rr   = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red, parity);
     const double init = sqrt(rr);
     double       res  = init;
     int          its  = 0;
     if (!(init < A.atol)) {
         double an = rr;
         for (int it = 1; it <= A.max_iter; ++it) {
-            rep_matvec(A, V, p_s, ap_s, pt_s, n, n3, cluster);
-            const double ad = owned_dot(ap_s, p_s, n, n3, rdiv, A.owned, red);
+            rep_matvec(A, V, p_s, ap_s, pt_s, xch, n, n3, cluster);
+            const double ad = owned_dot(ap_s, p_s, n, n3, rdiv, A.owned, red, parity);
             if (fabs(ad) < DBL_MIN) break;
             const double alpha = an / ad;
             for (int e = x0 + threadIdx.x; e < x1; e += blockDim.x) {
@@ -649,7 +716,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
             }
             for (int e = threadIdx.x; e < n3; e += blockDim.x) r_s[e] = r_s[e] - alpha * ap_s[e];
             __syncthreads();
-            rr  = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red);
+            rr  = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red, parity);
             res = sqrt(rr);
             its = it;
             if (res / init <= A.rtol || res < A.atol) break;

@@ -13,6 +13,8 @@
 // (x/2, y/2, r/2) + the fine wedge's node offset, with the reference's
 // shape_coarse(i, r%2, fine_lateral_wedge_idx(x, y, w)) weights; this keeps
 // B and B^T exact transposes of each other and of the reference.
+#include <algorithm>
+
 #include "tn_device.cuh"
 #include "tn_kernels.hpp"
 #include "tn_wedge_math.cuh"
@@ -61,6 +63,7 @@ struct CouplingArgs {
     int      nl, nr;  // fine level
     const T* coords;  // fine unit-sphere coords
     const T* colgeo;  // fine per-column wedge geometry (20 values per column)
+    const T* radgeo;  // fine per-radial-cell alpha, 1/(6 hdr), r_mid^2 hdr
     const T* radii;   // fine radii
     int      bc_cmb, bc_surf;
     const T* u[3];    // fine velocity (divergence input / gradient output)
@@ -110,192 +113,237 @@ __device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int 
 //        factorised velocity gradient of the epsilon-div-div kernel);
 //   B^T: -|det J_w| p_interp,w with p_interp the coarse-pressure interpolation
 //        at the fine wedge's centroid.
-// Pass 1 runs one thread per fine cell (r fastest); pass 2 distributes:
-// B adds the 16 fine wedges of a coarse cell into its 8 corners (8 atomics per
-// coarse cell), B^T gathers, per fine node, the up to 12 wedges around it
-// (no atomics, every node written once).
+// Pass 1 runs one thread per fine cell; pass 2 distributes: B adds the 16
+// fine wedges of a coarse cell into its 8 corners (8 atomics per coarse cell),
+// B^T gathers, per fine node, the up to 12 wedges around it (no atomics,
+// every node written once). Every kernel runs one CTA per lateral column
+// (grid = (y, x, diamond)) with threads along r, so the lateral geometry is
+// one broadcast per CTA and the radial factors come from the level's table.
 
-template <typename T>
-__device__ __forceinline__ void decode_cell(int cell, int nl, int nr, int& d, int& x, int& y, int& r)
-{
-    r     = cell % (nr - 1);
-    int t = cell / (nr - 1);
-    y     = t % (nl - 1);
-    t /= (nl - 1);
-    x = t % (nl - 1);
-    d = t / (nl - 1);
-}
+// Threads per CTA for n radial entries: whole warps, at most 256 (larger
+// columns loop).
+inline int radial_threads(int n) { return std::min(256, std::max(32, (n + 31) / 32 * 32)); }
 
+// The 10 geometry values of one wedge (e1, e2, e3, |det M|) by 2-wide loads:
+// the table's columns are 20 values and each wedge starts at a multiple of
+// 2 * sizeof(T) bytes.
 template <typename T>
-__global__ void __launch_bounds__(128) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <typename T>
+__device__ __forceinline__ void load_wedge_geo(const T* gw, T (&g)[10])
 {
-    const int nl = A.nl, nr = A.nr;
-    const int nc   = 10 * (nl - 1) * (nl - 1) * (nr - 1);
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= nc) return;
-    int d, x, y, r;
-    decode_cell<T>(cell, nl, nr, d, x, y, r);
-    const T*   G  = A.colgeo + static_cast<int64_t>(cell / (nr - 1)) * 20;
-    const T    r0 = A.radii[r], r1 = A.radii[r + 1];
-    const T    rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
-    const T    alpha = T(0.5) / rm, beta = T(1) / (T(6) * hdr);
-    const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
-    const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
-    const int  bside  = at_cmb ? 0 : 1;
-    // corner values u[q][s][c] with the boundary treatment of the wedge nodes
-    T u[4][2][3];
+    using V    = typename Pair<T>::type;
+    const V* v = reinterpret_cast<const V*>(gw);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int qx = x + (q & 1), qy = y + (q >> 1);
-#pragma unroll
-        for (int s2 = 0; s2 < 2; ++s2) {
-            const int64_t id = node_index(nl, nr, d, qx, qy, r + s2);
-            T             v0 = A.u[0][id], v1 = A.u[1][id], v2 = A.u[2][id];
-            if ((at_cmb || at_surf) && s2 == bside) {
-                if (bcf == 1) {
-                    v0 = v1 = v2 = T(0);
-                } else if (bcf == 2) {
-                    T nn[3];
-                    unit_normal<T>(A.coords, nl, d, qx, qy, nn);
-                    const T un = v0 * nn[0] + v1 * nn[1] + v2 * nn[2];
-                    v0 -= un * nn[0];
-                    v1 -= un * nn[1];
-                    v2 -= un * nn[2];
-                }
-            }
-            u[q][s2][0] = v0;
-            u[q][s2][1] = v1;
-            u[q][s2][2] = v2;
-        }
-    }
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-        const T*  gw = G + 10 * w;
-        const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
-        T         div = T(0);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const T S0 = u[q0][0][c] + u[q0][1][c], S1 = u[q1][0][c] + u[q1][1][c], S2 = u[q2][0][c] + u[q2][1][c];
-            const T Dc = (u[q0][1][c] - u[q0][0][c]) + (u[q1][1][c] - u[q1][0][c]) + (u[q2][1][c] - u[q2][0][c]);
-            div += alpha * (gw[c] * (S1 - S0) + gw[3 + c] * (S2 - S0)) + beta * gw[6 + c] * Dc;
-        }
-        wv[2 * static_cast<int64_t>(cell) + w] = -(gw[9] * rm * rm * hdr) * div;
+    for (int k = 0; k < 5; ++k) {
+        const V t    = __ldg(v + k);
+        g[2 * k]     = t.x;
+        g[2 * k + 1] = t.y;
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) div_scatter_kernel(CouplingArgs<T> A, const T* __restrict__ wv)
-{
-    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int ncc  = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= ncc) return;
-    int d, X, Y, R;
-    decode_cell<T>(cell, nlc, nrc, d, X, Y, R);
-    T acc[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] = T(0);
-#pragma unroll
-    for (int f = 0; f < 8; ++f) {
-        const int     x = 2 * X + (f & 1), y = 2 * Y + ((f >> 1) & 1), c = f >> 2, r = 2 * R + c;
-        const int64_t fc = node_index(nl - 1, nr - 1, d, x, y, r);
-#pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            const T   pre = wv[2 * fc + w];
-            const int flw = fine_lat_wedge(x, y, w);
-#pragma unroll
-            for (int i = 0; i < 6; ++i)
-                acc[woff(w, i, 0) + 2 * woff(w, i, 1) + 4 * woff(w, i, 2)] += pre * shape_coarse_centroid<T>(i, c, flw);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-        atomicAdd(&A.po[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))], acc[k]);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(128) grad_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
-{
-    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int nc   = 10 * (nl - 1) * (nl - 1) * (nr - 1);
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= nc) return;
-    int d, x, y, r;
-    decode_cell<T>(cell, nl, nr, d, x, y, r);
-    const T* G  = A.colgeo + static_cast<int64_t>(cell / (nr - 1)) * 20;
-    const T  r0 = A.radii[r], r1 = A.radii[r + 1];
-    const T  rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
-    const int X = x / 2, Y = y / 2, R = r / 2, frw = r & 1;
-    T         pc[8];  // coarse cell corner pressures
-#pragma unroll
-    for (int k = 0; k < 8; ++k) pc[k] = A.p[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))];
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-        const int flw = fine_lat_wedge(x, y, w);
-        T         pi  = T(0);
-#pragma unroll
-        for (int j = 0; j < 6; ++j)
-            pi += shape_coarse_centroid<T>(j, frw, flw) * pc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)];
-        wv[2 * static_cast<int64_t>(cell) + w] = -(G[10 * w + 9] * rm * rm * hdr) * pi;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(128) grad_gather_kernel(CouplingArgs<T> A, const T* __restrict__ wv, int add)
+__global__ void __launch_bounds__(256) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
 {
     const int     nl = A.nl, nr = A.nr;
-    const int64_t nn_total = 10ll * nl * nl * nr;
-    const int64_t node     = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (node >= nn_total) return;
-    const int r = static_cast<int>(node % nr);
-    int64_t   t = node / nr;
-    const int y = static_cast<int>(t % nl);
-    t /= nl;
-    const int  x = static_cast<int>(t % nl);
-    const int  d = static_cast<int>(t / nl);
-    const bool on_cmb = r == 0, on_surf = r == nr - 1;
-    const int  bcn    = on_cmb ? A.bc_cmb : (on_surf ? A.bc_surf : 0);
-    T          o[3]   = {T(0), T(0), T(0)};
-    if (bcn != 1) {
+    const int     y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
+    const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + x) * (nl - 1) + y;
+    T             gw[2][10];
+    load_wedge_geo<T>(A.colgeo + col * 20, gw[0]);
+    load_wedge_geo<T>(A.colgeo + col * 20 + 10, gw[1]);
+    int64_t base[4];
 #pragma unroll
-        for (int ab = 0; ab < 4; ++ab) {
-            const int a = ab & 1, b = ab >> 1;
-            const int xc = x - a, yc = y - b;
-            if (xc < 0 || yc < 0 || xc > nl - 2 || yc > nl - 2) continue;
-            const T*  G = A.colgeo + ((static_cast<int64_t>(d) * (nl - 1) + xc) * (nl - 1) + yc) * 20;
-            const int q = a + 2 * b;  // hex corner of the node in the cell
+    for (int q = 0; q < 4; ++q) base[q] = node_index(nl, nr, d, x + (q & 1), y + (q >> 1), 0);
+    for (int r = threadIdx.x; r < nr - 1; r += blockDim.x) {
+        const T    alpha = A.radgeo[3 * r], beta = A.radgeo[3 * r + 1], dfac = A.radgeo[3 * r + 2];
+        const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
+        const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
+        const int  bside  = at_cmb ? 0 : 1;
+        // corner values u[q][s][c] with the boundary treatment of the wedge nodes
+        T u[4][2][3];
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int rc = r - c;
-                if (rc < 0 || rc > nr - 2) continue;
-                const T       r0 = A.radii[rc], r1 = A.radii[rc + 1];
-                const T       rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
-                const T       alpha = T(0.5) / rm, sb = (c == 0 ? T(-1) : T(1)) / (T(6) * hdr);
-                const int64_t fc    = node_index(nl - 1, nr - 1, d, xc, yc, rc);
+        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const int64_t id = base[q] + r + s2;
+                T             v0 = A.u[0][id], v1 = A.u[1][id], v2 = A.u[2][id];
+                if ((at_cmb || at_surf) && s2 == bside) {
+                    if (bcf == 1) {
+                        v0 = v1 = v2 = T(0);
+                    } else if (bcf == 2) {
+                        T nn[3];
+                        unit_normal<T>(A.coords, nl, d, x + (q & 1), y + (q >> 1), nn);
+                        const T un = v0 * nn[0] + v1 * nn[1] + v2 * nn[2];
+                        v0 -= un * nn[0];
+                        v1 -= un * nn[1];
+                        v2 -= un * nn[2];
+                    }
+                }
+                u[q][s2][0] = v0;
+                u[q][s2][1] = v1;
+                u[q][s2][2] = v2;
+            }
+        }
+        T out[2];
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const T*  g  = gw[w];
+            const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
+            T         div = T(0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T S0 = u[q0][0][c] + u[q0][1][c], S1 = u[q1][0][c] + u[q1][1][c],
+                        S2 = u[q2][0][c] + u[q2][1][c];
+                const T Dc = (u[q0][1][c] - u[q0][0][c]) + (u[q1][1][c] - u[q1][0][c]) + (u[q2][1][c] - u[q2][0][c]);
+                div += alpha * (g[c] * (S1 - S0) + g[3 + c] * (S2 - S0)) + beta * g[6 + c] * Dc;
+            }
+            out[w] = -(g[9] * dfac) * div;
+        }
+        using V = typename Pair<T>::type;
+        V o;
+        o.x = out[0];
+        o.y = out[1];
+        reinterpret_cast<V*>(wv)[col * (nr - 1) + r] = o;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) div_scatter_kernel(CouplingArgs<T> A, const T* __restrict__ wv)
+{
+    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    const int Y = blockIdx.x, X = blockIdx.y, d = blockIdx.z;
+    using V     = typename Pair<T>::type;
+    for (int R = threadIdx.x; R < nrc - 1; R += blockDim.x) {
+        T acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = T(0);
+#pragma unroll
+        for (int f = 0; f < 8; ++f) {
+            const int     x = 2 * X + (f & 1), y = 2 * Y + ((f >> 1) & 1), c = f >> 2, r = 2 * R + c;
+            const int64_t fc = node_index(nl - 1, nr - 1, d, x, y, r);
+            const V       pv = reinterpret_cast<const V*>(wv)[fc];
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const T   pre = w == 0 ? pv.x : pv.y;
+                const int flw = fine_lat_wedge(x, y, w);
+#pragma unroll
+                for (int i = 0; i < 6; ++i)
+                    acc[woff(w, i, 0) + 2 * woff(w, i, 1) + 4 * woff(w, i, 2)] += pre * shape_coarse_centroid<T>(i, c, flw);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            atomicAdd(&A.po[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))], acc[k]);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) grad_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
+{
+    const int     nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    const int     y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
+    const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + x) * (nl - 1) + y;
+    const T       det0 = __ldg(A.colgeo + col * 20 + 9), det1 = __ldg(A.colgeo + col * 20 + 19);
+    const int     X = x / 2, Y = y / 2;
+    const int     flw0 = fine_lat_wedge(x, y, 0), flw1 = fine_lat_wedge(x, y, 1);
+    for (int r = threadIdx.x; r < nr - 1; r += blockDim.x) {
+        const T   dfac = A.radgeo[3 * r + 2];
+        const int R = r / 2, frw = r & 1;
+        T         pc[8];  // coarse cell corner pressures
+#pragma unroll
+        for (int k = 0; k < 8; ++k) pc[k] = A.p[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))];
+        T out[2];
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const int flw = w == 0 ? flw0 : flw1;
+            T         pi  = T(0);
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+                pi += shape_coarse_centroid<T>(j, frw, flw) * pc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)];
+            out[w] = -((w == 0 ? det0 : det1) * dfac) * pi;
+        }
+        using V = typename Pair<T>::type;
+        V o;
+        o.x = out[0];
+        o.y = out[1];
+        reinterpret_cast<V*>(wv)[col * (nr - 1) + r] = o;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) grad_gather_kernel(CouplingArgs<T> A, const T* __restrict__ wv, int add)
+{
+    const int nl = A.nl, nr = A.nr;
+    const int y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
+    using V     = typename Pair<T>::type;
+    const V* wv2 = reinterpret_cast<const V*>(wv);
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        const int64_t node    = node_index(nl, nr, d, x, y, r);
+        const bool    on_cmb  = r == 0, on_surf = r == nr - 1;
+        const int     bcn     = on_cmb ? A.bc_cmb : (on_surf ? A.bc_surf : 0);
+        T             o[3]    = {T(0), T(0), T(0)};
+        if (bcn != 1) {
+            // cell r above the node (node = its bottom, sign -1), cell r - 1 below (top, +1)
+            const bool up = r <= nr - 2, dn = r >= 1;
+            const T    al_up = up ? A.radgeo[3 * r] : T(0), sb_up = up ? -A.radgeo[3 * r + 1] : T(0);
+            const T    al_dn = dn ? A.radgeo[3 * (r - 1)] : T(0), sb_dn = dn ? A.radgeo[3 * (r - 1) + 1] : T(0);
+#pragma unroll
+            for (int ab = 0; ab < 4; ++ab) {
+                const int a = ab & 1, b = ab >> 1;
+                const int xc = x - a, yc = y - b;
+                if (xc < 0 || yc < 0 || xc > nl - 2 || yc > nl - 2) continue;
+                const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + xc) * (nl - 1) + yc;
+                const int     q   = a + 2 * b;  // hex corner of the node in the cell
+                const V       pu  = up ? wv2[col * (nr - 1) + r] : V{T(0), T(0)};
+                const V       pd  = dn ? wv2[col * (nr - 1) + r - 1] : V{T(0), T(0)};
 #pragma unroll
                 for (int w = 0; w < 2; ++w) {
                     const int m = w == 0 ? q : 3 - q;  // lateral index of corner q in wedge w
                     if (m > 2) continue;
-                    const T* gw  = G + 10 * w;
-                    const T  pre = wv[2 * fc + w];
+                    T g[10];
+                    load_wedge_geo<T>(A.colgeo + col * 20 + 10 * w, g);
+                    const T p_up = w == 0 ? pu.x : pu.y, p_dn = w == 0 ? pd.x : pd.y;
+                    const T ca = p_up * al_up + p_dn * al_dn;  // multiplies L_m
+                    const T cb = p_up * sb_up + p_dn * sb_dn;  // multiplies e3
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
-                        o[i] += pre * (alpha * L + sb * gw[6 + i]);
+                        const T L = m == 0 ? -(g[i] + g[3 + i]) : (m == 1 ? g[i] : g[3 + i]);
+                        o[i] += ca * L + cb * g[6 + i];
                     }
                 }
             }
-        }
-        if (bcn == 2) {
-            T nv[3];
-            unit_normal<T>(A.coords, nl, d, x, y, nv);
-            const T on = o[0] * nv[0] + o[1] * nv[1] + o[2] * nv[2];
+            if (bcn == 2) {
+                T nv[3];
+                unit_normal<T>(A.coords, nl, d, x, y, nv);
+                const T on = o[0] * nv[0] + o[1] * nv[1] + o[2] * nv[2];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) o[i] -= on * nv[i];
+                for (int i = 0; i < 3; ++i) o[i] -= on * nv[i];
+            }
         }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) A.uo[i][node] = add ? A.uo[i][node] + o[i] : o[i];
     }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) A.uo[i][node] = add ? A.uo[i][node] + o[i] : o[i];
+}
+
+// Radial factor table (one thread per radial cell).
+template <typename T>
+__global__ void radgeo_kernel(int nr, const T* radii, T* out)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nr - 1) return;
+    const T r0 = radii[r], r1 = radii[r + 1];
+    const T rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
+    out[3 * r]     = T(0.5) / rm;
+    out[3 * r + 1] = T(1) / (T(6) * hdr);
+    out[3 * r + 2] = rm * rm * hdr;
 }
 
 // Per-column wedge geometry table (column_geometry, 20 values per column).
@@ -421,6 +469,7 @@ static CouplingArgs<T> coupling_args(const CouplingLaunch<T>& p)
     a.nr      = p.nr;
     a.coords  = p.coords;
     a.colgeo  = p.colgeo;
+    a.radgeo  = p.radgeo;
     a.radii   = p.radii;
     a.bc_cmb  = p.bc_cmb;
     a.bc_surf = p.bc_surf;
@@ -437,12 +486,11 @@ template <typename T>
 int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t st)
 {
     if (!p.wedge_scratch) return -1;
+    if (!p.radgeo) return -1;
     const CouplingArgs<T> a   = coupling_args(p);
-    const int             nc  = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
     const int             nlc = (p.nl + 1) / 2, nrc = (p.nr + 1) / 2;
-    const int             ncc = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
-    div_cells_kernel<T><<<(nc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
-    div_scatter_kernel<T><<<(ncc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
+    div_cells_kernel<T><<<dim3(p.nl - 1, p.nl - 1, 10), radial_threads(p.nr - 1), 0, st>>>(a, p.wedge_scratch);
+    div_scatter_kernel<T><<<dim3(nlc - 1, nlc - 1, 10), radial_threads(nrc - 1), 0, st>>>(a, p.wedge_scratch);
     return launch_status(2);
 }
 
@@ -450,13 +498,21 @@ template <typename T>
 int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t st)
 {
     if (!p.wedge_scratch) return -1;
-    const CouplingArgs<T> a  = coupling_args(p);
-    const int             nc = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
-    const int64_t         n  = 10ll * p.nl * p.nl * p.nr;
-    grad_cells_kernel<T><<<(nc + 127) / 128, 128, 0, st>>>(a, p.wedge_scratch);
-    grad_gather_kernel<T><<<static_cast<int>((n + 127) / 128), 128, 0, st>>>(a, p.wedge_scratch, p.add);
+    if (!p.radgeo) return -1;
+    const CouplingArgs<T> a = coupling_args(p);
+    grad_cells_kernel<T><<<dim3(p.nl - 1, p.nl - 1, 10), radial_threads(p.nr - 1), 0, st>>>(a, p.wedge_scratch);
+    grad_gather_kernel<T><<<dim3(p.nl, p.nl, 10), radial_threads(p.nr), 0, st>>>(a, p.wedge_scratch, p.add);
     return launch_status(2);
 }
+
+template <typename T>
+int radial_geometry_table(int nr, const T* radii, T* out, cudaStream_t st)
+{
+    radgeo_kernel<T><<<(nr - 1 + 127) / 128, 128, 0, st>>>(nr, radii, out);
+    return launch_status();
+}
+template int radial_geometry_table<double>(int, const double*, double*, cudaStream_t);
+template int radial_geometry_table<float>(int, const float*, float*, cudaStream_t);
 
 template <typename T>
 int column_geometry_table(int nl, const T* coords, T* out, cudaStream_t st)

@@ -59,6 +59,7 @@ struct CouplingLaunch {
     int      nl = 0, nr = 0;  // fine (velocity) level
     const T* coords = nullptr;
     const T* colgeo = nullptr;  // per-column wedge geometry (column_geometry_table)
+    const T* radgeo = nullptr;  // per-radial-cell factors (radial_geometry_table)
     const T* radii  = nullptr;
     int      add    = 0;        // gradient: 1 accumulates into u_out, 0 overwrites
     T*       wedge_scratch = nullptr;  // 2 values per fine cell
@@ -70,6 +71,11 @@ struct CouplingLaunch {
 };
 // divergence accumulates into p_out (callers zero it for Replace); the
 // gradient writes (or with add accumulates into) every node of u_out.
+// Per radial cell rc of a level: alpha = 1/(2 r_mid), ib = 1/(6 hdr) and
+// dfac = r_mid^2 hdr (r_mid, hdr: mid radius and half height of the cell),
+// three values per cell.
+template <typename T>
+int radial_geometry_table(int nr, const T* radii, T* out, cudaStream_t stream);
 template <typename T>
 int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t stream);
 // e1, e2, e3 (columns of M^-T) and |det M| of both wedges of every lateral

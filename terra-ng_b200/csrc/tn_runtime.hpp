@@ -106,6 +106,7 @@ struct DeviceLevel {
     ShellLevel host;
     DevBuf     coords64, coords32;  // (10, nl, nl, 3)
     DevBuf     colgeo64, colgeo32;  // (10, nl-1, nl-1, 20) per-column wedge geometry
+    DevBuf     radgeo64, radgeo32;  // (nr-1, 3) per-radial-cell factors
     DevBuf     radii64, radii32;    // (nr)
     DevBuf     owned_lat;           // (10, nl, nl) uint8
     DevBuf     dup_offset, dup_members;
@@ -122,6 +123,8 @@ struct DeviceLevel {
     const T* radii() const;
     template <typename T>
     const T* colgeo() const;
+    template <typename T>
+    const T* radgeo() const;
 };
 template <>
 inline const double* DeviceLevel::coords<double>() const
@@ -142,6 +145,16 @@ template <>
 inline const float* DeviceLevel::colgeo<float>() const
 {
     return colgeo32.as<float>();
+}
+template <>
+inline const double* DeviceLevel::radgeo<double>() const
+{
+    return radgeo64.as<double>();
+}
+template <>
+inline const float* DeviceLevel::radgeo<float>() const
+{
+    return radgeo32.as<float>();
 }
 template <>
 inline const double* DeviceLevel::radii<double>() const

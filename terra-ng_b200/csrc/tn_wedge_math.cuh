@@ -269,12 +269,7 @@ __host__ __device__ __forceinline__ void hex_interior(const T (&u)[4][2][3], con
             S[q][c]  = u[q][0][c] + u[q][1][c];
             Dq[q][c] = u[q][1][c] - u[q][0][c];
         }
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) out[q][s][c] = T(0);
+    T v1w[2][3], v2w[2][3], wvw[2][3];
 #pragma unroll
     for (int w = 0; w < 2; ++w) {
         const T*  gw  = geo + 10 * w;
@@ -302,26 +297,35 @@ __host__ __device__ __forceinline__ void hex_interior(const T (&u)[4][2][3], con
         const T kd  = kw * (T(2) / T(3)) * (g00 + g11 + g22);
         const T s00 = k2 * g00 - kd, s11 = k2 * g11 - kd, s22 = k2 * g22 - kd;
         const T s01 = kw * h01, s02 = kw * h02, s12 = kw * h12;
-        T       v1[3], v2[3], wv[3];
-        v1[0] = s00 * E1[0] + s01 * E1[1] + s02 * E1[2];
-        v1[1] = s01 * E1[0] + s11 * E1[1] + s12 * E1[2];
-        v1[2] = s02 * E1[0] + s12 * E1[1] + s22 * E1[2];
-        v2[0] = s00 * E2[0] + s01 * E2[1] + s02 * E2[2];
-        v2[1] = s01 * E2[0] + s11 * E2[1] + s12 * E2[2];
-        v2[2] = s02 * E2[0] + s12 * E2[1] + s22 * E2[2];
-        wv[0] = s00 * E3[0] + s01 * E3[1] + s02 * E3[2];
-        wv[1] = s01 * E3[0] + s11 * E3[1] + s12 * E3[2];
-        wv[2] = s02 * E3[0] + s12 * E3[1] + s22 * E3[2];
+        v1w[w][0] = s00 * E1[0] + s01 * E1[1] + s02 * E1[2];
+        v1w[w][1] = s01 * E1[0] + s11 * E1[1] + s12 * E1[2];
+        v1w[w][2] = s02 * E1[0] + s12 * E1[1] + s22 * E1[2];
+        v2w[w][0] = s00 * E2[0] + s01 * E2[1] + s02 * E2[2];
+        v2w[w][1] = s01 * E2[0] + s11 * E2[1] + s12 * E2[2];
+        v2w[w][2] = s02 * E2[0] + s12 * E2[1] + s22 * E2[2];
+        wvw[w][0] = s00 * E3[0] + s01 * E3[1] + s02 * E3[2];
+        wvw[w][1] = s01 * E3[0] + s11 * E3[1] + s12 * E3[2];
+        wvw[w][2] = s02 * E3[0] + s12 * E3[1] + s22 * E3[2];
+    }
+    // Nodal outputs sigma g_n per corner: corner 0 is node m = 0 of wedge 0,
+    // corner 3 node m = 0 of wedge 1 (lateral part -(v1 + v2)); corner 1 is
+    // m = 1 of wedge 0 and m = 2 of wedge 1, corner 2 the reverse. The radial
+    // part (wv) enters the bottom node with -1 and the top node with +1.
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const T v12 = v1[c] + v2[c];
-            out[q0i][0][c] -= v12 + wv[c];
-            out[q0i][1][c] += wv[c] - v12;
-            out[q1i][0][c] += v1[c] - wv[c];
-            out[q1i][1][c] += v1[c] + wv[c];
-            out[q2i][0][c] += v2[c] - wv[c];
-            out[q2i][1][c] += v2[c] + wv[c];
-        }
+    for (int c = 0; c < 3; ++c) {
+        const T v120 = v1w[0][c] + v2w[0][c];
+        const T v121 = v1w[1][c] + v2w[1][c];
+        const T rad  = wvw[0][c] + wvw[1][c];
+        const T lat1 = v1w[0][c] + v2w[1][c];
+        const T lat2 = v2w[0][c] + v1w[1][c];
+        out[0][0][c] = -(v120 + wvw[0][c]);
+        out[0][1][c] = wvw[0][c] - v120;
+        out[3][0][c] = -(v121 + wvw[1][c]);
+        out[3][1][c] = wvw[1][c] - v121;
+        out[1][0][c] = lat1 - rad;
+        out[1][1][c] = lat1 + rad;
+        out[2][0][c] = lat2 - rad;
+        out[2][1][c] = lat2 + rad;
     }
 }
 

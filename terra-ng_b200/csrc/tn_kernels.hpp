@@ -200,7 +200,9 @@ struct AxpyList {
 struct CoarsePcgArgs {
     int            nl = 0, nr = 0;
     const double*  mats        = nullptr;  // baked stored matrices of the level
+    const double*  mats_full   = nullptr;  // row-major copy (coarse_matrices_unpack), for the replicated kernel
     int            num_classes = 0;
+    int            num_members = 0;  // off[num_classes]
     const int32_t* off = nullptr;
     const int32_t* mem = nullptr;
     const uint8_t* owned = nullptr;
@@ -253,7 +255,12 @@ int flag_nonfinite(int64_t n, const T* a, int* flag_dev, cudaStream_t st);
 int widen_check(int64_t n, const float* in, double* out, int* flag_dev, cudaStream_t st);
 int coarse_pcg(const CoarsePcgArgs& args, cudaStream_t st);
 // decide and cache the launch configuration for a level (call outside graph capture)
-int coarse_pcg_prepare(int nl, int nr);
+int coarse_pcg_prepare(int nl, int nr, int num_classes, int num_members);
+// 1 when the coarsest CG of this level runs the replicated kernel, which reads
+// the row-major matrix copy made by coarse_matrices_unpack
+int coarse_pcg_uses_full_matrices(int nl, int nr, int num_classes, int num_members);
+// full[(w * 18 + a) * 18 + b][cell] = packed[w * 171 + pidx(a, b)][cell], nc cells
+int coarse_matrices_unpack(int nc, const double* packed, double* full, cudaStream_t st);
 int coarse_pcg_partials_size();
 int coarse_pcg_cluster_size();
 

@@ -103,6 +103,7 @@ class VelocityMultigrid {
     Work<float>                               w32_;
     DVec<double>                              cx_, cb_, cr_, cp_, cap_;  // coarsest CG vectors
     DevBuf                                    cpart_, cstats_;
+    DevBuf                                    cfull_;  // row-major coarsest matrices (replicated CG)
     DVec<double>                              ext64_[2];
     DVec<float>                               ext32_[2];
 };

@@ -122,33 +122,9 @@ __device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int 
 
 // Flat grids of 256 threads, one thread per fine cell / coarse cell / fine
 // node in storage order (r fastest), so warps read consecutive radial
-// entries and no thread idles. Indices are decoded with exact reciprocal
-// multiplications: q = (i * (floor(2^40 / n) + 1)) >> 40 equals i / n for
-// 0 <= i < 2^40 / n, far above any level's entry count.
+// entries and no thread idles; indices are decoded with Decoder (exact
+// reciprocal multiplications).
 constexpr int kCouplingThreads = 256;
-
-struct Decoder {
-    int      n;
-    uint64_t m;
-    __host__ __device__ Decoder() : n(1), m(0) {}
-    explicit Decoder(int n_) : n(n_), m(reciprocal_nr(n_)) {}
-    __device__ __forceinline__ int div(int i) const
-    {
-        return static_cast<int>((static_cast<uint64_t>(static_cast<uint32_t>(i)) * m) >> 40);
-    }
-};
-
-// i = ((d * nlat + x) * nlat + y) * nrad + r
-__device__ __forceinline__ void decode4(int i, const Decoder& rad, const Decoder& lat, int& d, int& x, int& y, int& r,
-                                        int& col)
-{
-    col          = rad.div(i);
-    r            = i - col * rad.n;
-    const int dx = lat.div(col);
-    y            = col - dx * lat.n;
-    d            = lat.div(dx);
-    x            = dx - d * lat.n;
-}
 
 template <typename T>
 struct Pair;
@@ -161,12 +137,13 @@ struct Pair<float> {
     using type = float2;
 };
 
-// B, pass 1: one thread per fine cell, one velocity component at a time so
-// only that component's 8 corner values are live (low register use keeps the
-// SM full of warps, which this latency-bound gather needs).
+// B, pass 1: one thread per fine cell. All 24 corner values are loaded
+// before any arithmetic (the kernel is bound by load latency, so every load
+// of a cell is in flight at once); the lateral geometry is read from L1 where
+// it is used rather than held in registers.
 template <typename T>
-__global__ void __launch_bounds__(kCouplingThreads, 4) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv, int nc,
-                                                                     Decoder rad, Decoder lat)
+__global__ void __launch_bounds__(kCouplingThreads) div_cells_kernel(CouplingArgs<T> A, T* __restrict__ wv, int nc,
+                                                                        Decoder rad, Decoder lat)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nc) return;
@@ -174,59 +151,57 @@ __global__ void __launch_bounds__(kCouplingThreads, 4) div_cells_kernel(Coupling
     int       d, x, y, r, col;
     decode4(i, rad, lat, d, x, y, r, col);
     const T* G = A.colgeo + static_cast<int64_t>(col) * 20;
-    // node offsets fit in 32 bits (10 nl^2 nr < 2^31 up to level 8)
-    int base[4];
+    T        u[4][2][3];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) base[q] = static_cast<int>(node_index(nl, nr, d, x + (q & 1), y + (q >> 1), r));
-    const T    alpha = A.radgeo[3 * r], beta = A.radgeo[3 * r + 1], dfac = A.radgeo[3 * r + 2];
+    for (int q = 0; q < 4; ++q) {
+        // node offsets fit in 32 bits (10 nl^2 nr < 2^31 up to level 8)
+        const int id = static_cast<int>(node_index(nl, nr, d, x + (q & 1), y + (q >> 1), r));
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) u[q][s2][c] = A.u[c][id + s2];
+    }
     const bool at_cmb = r == 0, at_surf = r + 1 == nr - 1;
     const int  bcf    = at_cmb ? A.bc_cmb : (at_surf ? A.bc_surf : 0);
-    const int  bside  = at_cmb ? 0 : 1;
-    // boundary side: Dirichlet drops the values, free-slip their normal part
-    // (n.u per corner here, the normal's components re-read below)
-    T un[4] = {T(0), T(0), T(0), T(0)};
-    if (bcf == 2) {
+    if (bcf == 1 || bcf == 2) {
+        const int bside = at_cmb ? 0 : 1;
+        // compile-time side index (a runtime index would move u to local memory)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            T nq[3];
-            unit_normal<T>(A.coords, nl, d, x + (q & 1), y + (q >> 1), nq);
-            const int id = base[q] + bside;
-            un[q]        = A.u[0][id] * nq[0] + A.u[1][id] * nq[1] + A.u[2][id] * nq[2];
-        }
-    }
-    T div[2] = {T(0), T(0)};
+        for (int sd = 0; sd < 2; ++sd) {
+            if (sd != bside) continue;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        T S[4], D[4];
+            for (int q = 0; q < 4; ++q) {
+                if (bcf == 1) {
+                    u[q][sd][0] = u[q][sd][1] = u[q][sd][2] = T(0);
+                } else {
+                    T nn[3];
+                    unit_normal<T>(A.coords, nl, d, x + (q & 1), y + (q >> 1), nn);
+                    const T un = u[q][sd][0] * nn[0] + u[q][sd][1] * nn[1] + u[q][sd][2] * nn[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            T v[2];
-#pragma unroll
-            for (int s2 = 0; s2 < 2; ++s2) {
-                v[s2] = A.u[c][base[q] + s2];
-                if (bcf != 0 && s2 == bside) {
-                    if (bcf == 1)
-                        v[s2] = T(0);
-                    else if (bcf == 2)
-                        v[s2] -= un[q] * A.coords[lat_index3(nl, d, x + (q & 1), y + (q >> 1)) * 3 + c];
+                    for (int c = 0; c < 3; ++c) u[q][sd][c] -= un * nn[c];
                 }
             }
-            S[q] = v[0] + v[1];
-            D[q] = v[1] - v[0];
         }
+    }
+    const T alpha = A.radgeo[3 * r], beta = A.radgeo[3 * r + 1], dfac = A.radgeo[3 * r + 2];
+    T       out[2];
 #pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            const T*  g  = G + 10 * w;
-            const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
-            const T   Dc = D[q0] + D[q1] + D[q2];
-            div[w] += alpha * (__ldg(g + c) * (S[q1] - S[q0]) + __ldg(g + 3 + c) * (S[q2] - S[q0])) +
-                      beta * __ldg(g + 6 + c) * Dc;
+    for (int w = 0; w < 2; ++w) {
+        const T*  g  = G + 10 * w;
+        const int q0 = wedge_corner(w, 0), q1 = wedge_corner(w, 1), q2 = wedge_corner(w, 2);
+        T         div = T(0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T S0 = u[q0][0][c] + u[q0][1][c], S1 = u[q1][0][c] + u[q1][1][c], S2 = u[q2][0][c] + u[q2][1][c];
+            const T Dc = (u[q0][1][c] - u[q0][0][c]) + (u[q1][1][c] - u[q1][0][c]) + (u[q2][1][c] - u[q2][0][c]);
+            div += alpha * (__ldg(g + c) * (S1 - S0) + __ldg(g + 3 + c) * (S2 - S0)) + beta * __ldg(g + 6 + c) * Dc;
         }
+        out[w] = -(__ldg(g + 9) * dfac) * div;
     }
     using V = typename Pair<T>::type;
     V o;
-    o.x                            = -(__ldg(G + 9) * dfac) * div[0];
-    o.y                            = -(__ldg(G + 19) * dfac) * div[1];
+    o.x                         = out[0];
+    o.y                         = out[1];
     reinterpret_cast<V*>(wv)[i] = o;
 }
 

@@ -180,6 +180,33 @@ struct VecSeg {
 #define TN_HOST_DEVICE
 #endif
 TN_HOST_DEVICE inline uint64_t reciprocal_nr(int nr) { return (uint64_t(1) << 40) / static_cast<uint64_t>(nr) + 1; }
+
+// Exact division by a fixed n through one multiply and shift:
+// (i * (floor(2^40 / n) + 1)) >> 40 == i / n for 0 <= i < 2^40 / n, far above
+// any level's entry count. Used to decode flat thread indices.
+struct Decoder {
+    int      n = 1;
+    uint64_t m = 0;
+    Decoder() = default;
+    explicit Decoder(int n_) : n(n_), m(reciprocal_nr(n_)) {}
+    TN_HOST_DEVICE int div(int i) const
+    {
+        return static_cast<int>((static_cast<uint64_t>(static_cast<uint32_t>(i)) * m) >> 40);
+    }
+};
+
+// i = ((d * nlat + x) * nlat + y) * nrad + r  ->  (d, x, y, r) and the lateral
+// column index (d * nlat + x) * nlat + y
+TN_HOST_DEVICE inline void decode4(int i, const Decoder& rad, const Decoder& lat, int& d, int& x, int& y, int& r,
+                                   int& col)
+{
+    col          = rad.div(i);
+    r            = i - col * rad.n;
+    const int dx = lat.div(col);
+    y            = col - dx * lat.n;
+    d            = lat.div(dx);
+    x            = dx - d * lat.n;
+}
 struct VecDesc {
     int     nseg = 0;
     VecSeg  seg[2];

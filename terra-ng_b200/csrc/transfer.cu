@@ -25,13 +25,20 @@ struct PtrSet {
     T*       out[kMaxComp];
 };
 
+// Flat grids: one thread per fine node (prolongation) or coarse node
+// (restriction) in storage order, 256 threads per CTA, indices decoded with
+// Decoder, so no thread of a radial column idles.
+constexpr int kTransferThreads = 256;
+
 template <typename T>
-__global__ void prolongate_kernel(int nlf, int nrf, int ncomp, PtrSet<T> P)
+__global__ void __launch_bounds__(kTransferThreads) prolongate_kernel(int nlf, int nrf, int ncomp, PtrSet<T> P, int n,
+                                                                      Decoder rad, Decoder lat)
 {
     const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
-    const int r   = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y   = blockIdx.y % nlf, x = blockIdx.y / nlf, d = blockIdx.z;
-    if (r >= nrf) return;
+    const int i   = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int d, x, y, r, col;
+    decode4(i, rad, lat, d, x, y, r, col);
     // lateral parents (at most two) with weights
     int xa[2], ya[2], nlat;
     if ((x & 1) == 0 && (y & 1) == 0) {
@@ -62,7 +69,7 @@ __global__ void prolongate_kernel(int nlf, int nrf, int ncomp, PtrSet<T> P)
         nrad  = 2;
     }
     const T       wr = nrad == 1 ? T(1) : T(0.5);
-    const int64_t fi = node_index(nlf, nrf, d, x, y, r);
+    const int64_t fi = i;
     for (int c = 0; c < ncomp; ++c) {
         T acc = T(0);
         for (int a = 0; a < nlat; ++a)
@@ -72,12 +79,15 @@ __global__ void prolongate_kernel(int nlf, int nrf, int ncomp, PtrSet<T> P)
 }
 
 template <typename T>
-__global__ void restrict_kernel(int nlf, int nrf, int ncomp, const uint8_t* __restrict__ owned, PtrSet<T> P)
+__global__ void __launch_bounds__(kTransferThreads) restrict_kernel(int nlf, int nrf, int ncomp,
+                                                                    const uint8_t* __restrict__ owned, PtrSet<T> P,
+                                                                    int n, Decoder rad, Decoder lat)
 {
     const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
-    const int rc  = blockIdx.x * blockDim.x + threadIdx.x;
-    const int yc  = blockIdx.y % nlc, xc = blockIdx.y / nlc, d = blockIdx.z;
-    if (rc >= nrc) return;
+    const int i   = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int d, xc, yc, rc, col;
+    decode4(i, rad, lat, d, xc, yc, rc, col);
     // 7-point lateral stencil (prolongation_constant_fine_grid_stencil_offsets_at_coarse_vertex)
     constexpr int ox[7] = {-1, -1, 0, 1, 1, 0, 0};
     constexpr int oy[7] = {0, 1, 1, 0, -1, -1, 0};
@@ -98,7 +108,7 @@ __global__ void restrict_kernel(int nlf, int nrf, int ncomp, const uint8_t* __re
             for (int c = 0; c < ncomp; ++c) acc[c] += wgt * P.in[c][fi];
         }
     }
-    const int64_t ci = node_index(nlc, nrc, d, xc, yc, rc);
+    const int64_t ci = i;
     for (int c = 0; c < ncomp; ++c) P.out[c][ci] = acc[c];
 }
 
@@ -119,8 +129,9 @@ int prolongate_add(int nlf, int nrf, int ncomp, const T* const* coarse, T* const
         P.in[c]  = coarse[c];
         P.out[c] = fine[c];
     }
-    const int thr = nrf >= 64 ? 64 : 32;
-    prolongate_kernel<T><<<dim3((nrf + thr - 1) / thr, nlf * nlf, 10), thr, 0, st>>>(nlf, nrf, ncomp, P);
+    const int n = 10 * nlf * nlf * nrf;
+    prolongate_kernel<T><<<(n + kTransferThreads - 1) / kTransferThreads, kTransferThreads, 0, st>>>(
+        nlf, nrf, ncomp, P, n, Decoder(nrf), Decoder(nlf));
     return launch_status();
 }
 
@@ -135,8 +146,9 @@ int restrict_owned(int nlf, int nrf, int ncomp, const uint8_t* owned_lat_fine, c
         P.out[c] = coarse[c];
     }
     const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
-    const int thr = nrc >= 64 ? 64 : 32;
-    restrict_kernel<T><<<dim3((nrc + thr - 1) / thr, nlc * nlc, 10), thr, 0, st>>>(nlf, nrf, ncomp, owned_lat_fine, P);
+    const int n = 10 * nlc * nlc * nrc;
+    restrict_kernel<T><<<(n + kTransferThreads - 1) / kTransferThreads, kTransferThreads, 0, st>>>(
+        nlf, nrf, ncomp, owned_lat_fine, P, n, Decoder(nrc), Decoder(nlc));
     return launch_status();
 }
 

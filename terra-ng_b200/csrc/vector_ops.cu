@@ -5,6 +5,8 @@
 // (kernels/common/grid_operations.hpp:132-346, communication_plan.hpp:471-517);
 // here each operation is one launch over all components, and the interface
 // sum is one gather-sum launch over the precomputed duplicate classes.
+#include <algorithm>
+
 #include "tn_device.cuh"
 #include "tn_kernels.hpp"
 
@@ -24,20 +26,41 @@ struct CComps {
 
 // ---------------------------------------------------------------------------
 // Interface sum: every member of a duplicate class receives the class sum.
-// One thread per (class, r); members are read along r (coalesced).
+// One thread per (class, r, component); members are read along r (coalesced).
+// A class has at most 5 members (the poles); their values are loaded before
+// the sum so the loads overlap, and summed in member order.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void iface_kernel(int num_classes, const int32_t* __restrict__ off, const int32_t* __restrict__ mem, int nr,
                              int ncomp, Comps<T> v)
 {
     const int cls = blockIdx.x;
+    const int c   = blockIdx.z;
     const int r   = blockIdx.y * blockDim.x + threadIdx.x;
-    if (cls >= num_classes || r >= nr) return;
-    const int b = off[cls], e = off[cls + 1];
-    for (int c = 0; c < ncomp; ++c) {
+    if (cls >= num_classes || r >= nr || c >= ncomp) return;
+    const int b = __ldg(off + cls), e = __ldg(off + cls + 1);
+    T*        p = v.p[c];
+    constexpr int kMax = 8;
+    if (e - b <= kMax) {
+        int64_t idx[kMax];
+        T       val[kMax];
+#pragma unroll
+        for (int k = 0; k < kMax; ++k)
+            if (b + k < e) idx[k] = static_cast<int64_t>(__ldg(mem + b + k)) * nr + r;
+#pragma unroll
+        for (int k = 0; k < kMax; ++k)
+            if (b + k < e) val[k] = p[idx[k]];
         T s = T(0);
-        for (int m = b; m < e; ++m) s += v.p[c][static_cast<int64_t>(mem[m]) * nr + r];
-        for (int m = b; m < e; ++m) v.p[c][static_cast<int64_t>(mem[m]) * nr + r] = s;
+#pragma unroll
+        for (int k = 0; k < kMax; ++k)
+            if (b + k < e) s += val[k];
+#pragma unroll
+        for (int k = 0; k < kMax; ++k)
+            if (b + k < e) p[idx[k]] = s;
+    } else {
+        T s = T(0);
+        for (int m = b; m < e; ++m) s += p[static_cast<int64_t>(mem[m]) * nr + r];
+        for (int m = b; m < e; ++m) p[static_cast<int64_t>(mem[m]) * nr + r] = s;
     }
 }
 
@@ -205,8 +228,8 @@ int interface_sum(const IfaceTable& t, int nr, int ncomp, T* const* comps, cudaS
     if (t.num_classes == 0) return 0;
     Comps<T> v{};
     for (int c = 0; c < ncomp; ++c) v.p[c] = comps[c];
-    const int threads = nr >= 64 ? 64 : 32;
-    dim3      grid(t.num_classes, (nr + threads - 1) / threads);
+    const int threads = std::min(256, (nr + 31) / 32 * 32);
+    dim3      grid(t.num_classes, (nr + threads - 1) / threads, ncomp);
     iface_kernel<T><<<grid, threads, 0, stream>>>(t.num_classes, t.offset, t.members, nr, ncomp, v);
     return launch_status();
 }

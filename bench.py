@@ -646,7 +646,10 @@ def run_adjoint_l5(a):
         gr = torch.zeros(theta.shape, dtype=torch.float64, device=dev)
         ok = s.misfit_gradient(x, u_obs, gr)
         a_its, a_res, _ = s.result()
-        adj14[name] = {"converged": bool(ok), "iterations": a_its, "relative_residual": a_res}
+        hist = s.history()
+        adj14[name] = {"converged": bool(ok), "iterations": a_its, "relative_residual": a_res,
+                       "first_iteration_below": {f"{t:g}": next((i for i, v in enumerate(hist) if v <= t), None)
+                                                 for t in (1e-4, 1e-6, 1e-8, 1e-10)}}
         grads[name] = gr.cpu().numpy()
         del s
     gm, gd = grads["mixed"], grads["fp64"]

@@ -70,10 +70,18 @@ __global__ void __launch_bounds__(kTransferThreads) prolongate_kernel(int nlf, i
     }
     const T       wr = nrad == 1 ? T(1) : T(0.5);
     const int64_t fi = i;
+    // Copies of a diamond-edge node in different diamonds list their two
+    // lateral parents in different orders. Summing the lateral pair first
+    // (a two-term sum is the same in either order) and then the radial pair
+    // (same order everywhere) gives every copy identical bits, so prolonged
+    // vectors stay consistent on interface duplicates in FP32 as in FP64.
     for (int c = 0; c < ncomp; ++c) {
         T acc = T(0);
-        for (int a = 0; a < nlat; ++a)
-            for (int b = 0; b < nrad; ++b) acc += P.in[c][node_index(nlc, nrc, d, xa[a], ya[a], ra[b])];
+        for (int b = 0; b < nrad; ++b) {
+            T lat = P.in[c][node_index(nlc, nrc, d, xa[0], ya[0], ra[b])];
+            if (nlat == 2) lat += P.in[c][node_index(nlc, nrc, d, xa[1], ya[1], ra[b])];
+            acc += lat;
+        }
         P.out[c][fi] += wl * wr * acc;
     }
 }

@@ -328,9 +328,23 @@ def test_stokes_preconditioner_matches_oracle(cuda):
     assert rel_err(z[3].cpu().numpy(), zp) < 1e-12
 
 
+def _max_duplicate_spread(g, level, v):
+    """Largest difference between copies of one node (v: (ncomp, 10, nl, nl, nr))."""
+    cls, n = g.duplicate_classes(level)
+    flat = cls.reshape(-1)
+    vv = v.reshape(v.shape[0], -1, v.shape[-1])
+    spread = 0.0
+    for k in range(n):
+        idx = np.where(flat == k)[0]
+        spread = max(spread, float(np.abs(vv[:, idx] - vv[:, idx[:1]]).max()))
+    return spread
+
+
 def test_stokes_mixed_precision_reaches_tolerance(cuda):
     """FP32 V-cycle inside FP64 FGMRES reaches the same 1e-8 relative residual;
-    the solution is compared with the FP64 solve."""
+    the solution is compared with the FP64 solve. Both solutions hold bitwise
+    equal values on every copy of an interface node (a solution used as the
+    data of another solve, e.g. an adjoint right-hand side, must be consistent)."""
     import torch
 
     level, nlev, bcs = 4, 3, (1, 1)
@@ -348,6 +362,8 @@ def test_stokes_mixed_precision_reaches_tolerance(cuda):
         its, rr, conv = solver.result()
         assert conv and rr <= 1e-8
         sols.append((np.stack([x[c].cpu().numpy() for c in range(3)]), x[3].cpu().numpy(), its))
+        assert _max_duplicate_spread(g, nlev - 1, sols[-1][0]) == 0.0
+        assert _max_duplicate_spread(g, nlev - 2, sols[-1][1][None]) == 0.0
     (u64, p64, it64), (u32, p32, it32) = sols
     assert it32 <= 1.25 * it64 + 5
     # both stop at a 1e-8 residual, so they agree to the problem's conditioning

@@ -72,32 +72,6 @@ struct CouplingArgs {
     T*       po;      // coarse pressure (divergence output)
 };
 
-// Per-cell physical gradients of the six wedge nodes for both wedges.
-template <typename T>
-__device__ __forceinline__ void cell_grads(const T* coords, int nl, int d, int x, int y, T r0, T r1, T (&g)[2][6][3],
-                                           T (&absdet)[2])
-{
-    T geo[20];
-    column_geometry<T>(coords, nl, d, x, y, geo);
-    const T rm = T(0.5) * (r0 + r1), hdr = T(0.5) * (r1 - r0);
-    const T alpha = T(0.5) / rm, beta = T(1) / (T(6) * hdr);
-#pragma unroll
-    for (int w = 0; w < 2; ++w) {
-        const T* gw = geo + 10 * w;
-        absdet[w]   = gw[9] * rm * rm * hdr;
-#pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            const int m  = n % 3;
-            const T   sg = n < 3 ? T(-1) : T(1);
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const T L = m == 0 ? -(gw[i] + gw[3 + i]) : (m == 1 ? gw[i] : gw[3 + i]);
-                g[w][n][i] = alpha * L + sg * beta * gw[6 + i];
-            }
-        }
-    }
-}
-
 template <typename T>
 __device__ __forceinline__ void unit_normal(const T* coords, int nl, int d, int x, int y, T (&n)[3])
 {

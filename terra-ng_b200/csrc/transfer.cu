@@ -91,8 +91,7 @@ __global__ void __launch_bounds__(kTransferThreads) restrict_kernel(int nlf, int
                                                                     const uint8_t* __restrict__ owned, PtrSet<T> P,
                                                                     int n, Decoder rad, Decoder lat)
 {
-    const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
-    const int i   = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int d, xc, yc, rc, col;
     decode4(i, rad, lat, d, xc, yc, rc, col);

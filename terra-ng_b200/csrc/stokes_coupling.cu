@@ -7,9 +7,11 @@
 //   lumped k-mass  : diag of the 6-point k-weighted pressure mass (kmass.hpp:98-181)
 //   vector mass    : 6-point mass matrix applied per component (vector_mass.hpp:60-150)
 //
-// One thread per fine cell (threads along r), both wedges, factorised wedge
-// Jacobian as in the epsilon-div-div kernel, contributions added with native
-// FP64/FP32 global atomics. The coarse node of fine wedge node i is
+// B and B^T run in two passes through one scalar per fine wedge (described
+// before the kernels below) on flat grids, with the factorised wedge Jacobian
+// of the epsilon-div-div kernel from per-level geometry tables. The mass
+// matrices run one thread per fine cell and add with native FP64/FP32 global
+// atomics (set-up only). The coarse node of fine wedge node i is
 // (x/2, y/2, r/2) + the fine wedge's node offset, with the reference's
 // shape_coarse(i, r%2, fine_lateral_wedge_idx(x, y, w)) weights; this keeps
 // B and B^T exact transposes of each other and of the reference.

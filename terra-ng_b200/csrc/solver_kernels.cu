@@ -97,8 +97,9 @@ __global__ void __launch_bounds__(kThreads) vdot_kernel(VecDesc L, const T* __re
 // w once per basis vector; w (the level-6 Stokes vector is 69 MB) fits in the
 // 126 MB L2 while the basis vectors stream past it. w is loaded and stored
 // with an evict_last policy and the basis vectors with streaming loads, so
-// each step costs about one basis-vector read of DRAM traffic instead of two
-// vectors plus w. The last step of an Arnoldi iteration (the norm) stores w
+// each step reads the two basis vectors it uses (v_{i-1}, partly still in L2
+// from the step before, and v_i) from DRAM, instead of those two plus w read
+// and written. The last step of an Arnoldi iteration (the norm) stores w
 // with evict_normal, which hands the lines back to ordinary replacement before
 // the preconditioner runs.
 __device__ __forceinline__ uint64_t l2_policy(bool keep)

@@ -241,7 +241,14 @@ typedef struct tn_solver_options {
                                            constant pressure as a null vector; not in the reference (0) */
     int      cuda_graphs;               /* Stokes: capture each Arnoldi step once and replay it as a CUDA
                                            graph (1) */
+    int      smoother;                  /* multigrid smoother: TN_SMOOTHER_CHEBYSHEV (Chebyshev::solve_impl,
+                                           chebyshev.hpp:102-176) or TN_SMOOTHER_JACOBI (damped Jacobi,
+                                           Jacobi::solve_impl, jacobi.hpp:51-60, chebyshev_iterations steps)
+                                           (TN_SMOOTHER_CHEBYSHEV) */
+    double   jacobi_omega;              /* damped-Jacobi relaxation omega (1.0, the reference's default) */
 } tn_solver_options;
+#define TN_SMOOTHER_CHEBYSHEV 0
+#define TN_SMOOTHER_JACOBI 1
 void tn_solver_options_default(tn_solver_options* opts);
 /* Stokes solve on velocity_level / velocity_level-1 (StokesContext,
  * apps/mantlecirculation/src/stokes_solver.hpp:325-609): FGMRES(m) with the

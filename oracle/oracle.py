@@ -385,6 +385,21 @@ class Chebyshev:
         return x
 
 
+@dataclass
+class Jacobi:
+    """Damped Jacobi smoother (jacobi.hpp:51-60): x += omega D^-1 (b - A x),
+    `iterations` times."""
+
+    inv_diag: np.ndarray
+    iterations: int = 1
+    omega: float = 1.0
+
+    def solve(self, A, x, b):
+        for _ in range(self.iterations):
+            x = x + self.omega * ((b - A(x)) * self.inv_diag)
+        return x
+
+
 def pcg(A, x, b, dot, max_iter, rtol, atol=1e-16, precond=None, history=None):
     """pcg.hpp:81-169. ``precond(z, r)`` returns the new z; like the
     reference's solve(preconditioner_, A, z_, r_) it receives the previous z
@@ -609,10 +624,13 @@ class VelocityHierarchy:
     def power_iteration(self, l, start, iterations):
         return power_iteration(lambda v: self.apply(l, v) * self.inv_diag[l], start, self.shells[l].dot, iterations)
 
-    def multigrid(self, num_cycles=1):
+    def multigrid(self, num_cycles=1, smoother="chebyshev", omega=1.0):
         n = len(self.shells)
-        smoothers = [None] + [Chebyshev(self.cheb_order, self.inv_diag[l], self.cheb_iters, self.lambdas[l])
-                              for l in range(1, n)]
+        if smoother == "jacobi":
+            smoothers = [None] + [Jacobi(self.inv_diag[l], self.cheb_iters, omega) for l in range(1, n)]
+        else:
+            smoothers = [None] + [Chebyshev(self.cheb_order, self.inv_diag[l], self.cheb_iters, self.lambdas[l])
+                                  for l in range(1, n)]
         ops = [(lambda v, l=l: self.apply(l, v)) for l in range(n)]
         it, rtol, atol = self.coarse
         coarse = lambda A, x, b: pcg(A, x, b, self.shells[0].dot, it, rtol, atol)

@@ -110,7 +110,11 @@ tn::MgOptions mg_options(const tn_solver_options& o)
     m.gca             = o.gca;
     m.fp32            = o.mixed_precision != 0;
     m.seed            = o.seed;
+    m.smoother        = o.smoother;
+    m.jacobi_omega    = o.jacobi_omega;
     need(o.gca == 0 || o.gca == 1, "gca must be 0 or 1");
+    need(o.smoother == TN_SMOOTHER_CHEBYSHEV || o.smoother == TN_SMOOTHER_JACOBI, "unknown smoother");
+    need(o.jacobi_omega > 0.0, "jacobi_omega must be positive");
     return m;
 }
 
@@ -640,6 +644,8 @@ void tn_solver_options_default(tn_solver_options* o)
     o->normalize_pressure        = 1;
     o->project_pressure_mean     = 0;
     o->cuda_graphs               = 1;
+    o->smoother                  = TN_SMOOTHER_CHEBYSHEV;
+    o->jacobi_omega              = 1.0;
 }
 
 int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,

@@ -140,7 +140,8 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     if (fine.stored) throw Error(kErrUnsupported, "the finest multigrid operator must be matrix-free");
     if (fine.precision != 0) throw Error(kErrArg, "the multigrid hierarchy is built from an FP64 operator");
     if (fine_ < 1) throw Error(kErrArg, "multigrid needs at least two levels");
-    if (o.cheb_order < 1 || o.cheb_iters < 0 || o.num_vcycles < 1 || o.coarse_max_iter < 0)
+    if (o.cheb_order < 1 || o.cheb_iters < 0 || o.num_vcycles < 1 || o.coarse_max_iter < 0 ||
+        (o.smoother != 0 && o.smoother != 1) || !(o.jacobi_omega > 0.0))
         throw Error(kErrArg, "invalid multigrid options");
     const int nlev = fine_ + 1;
     ops64_.resize(nlev);
@@ -262,7 +263,9 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
         chk(lincomb<double>(L.nodes(), 3, o3, 0.0, 0, nullptr, nullptr, nullptr, nullptr, st), "zero");
     }
     // Chebyshev spectrum estimates (chebyshev.hpp estimate_max_eigenvalues)
-    for (int l = 1; l <= fine_; ++l) lambda_[l] = power_iteration(l, o.power_iters, o.seed + 7919ull * l, st);
+    // lambda_max of D^-1 A per level for the Chebyshev smoother (the Jacobi smoother needs none)
+    if (o.smoother == 0)
+        for (int l = 1; l <= fine_; ++l) lambda_[l] = power_iteration(l, o.power_iters, o.seed + 7919ull * l, st);
     // one FP32 apply per level now: kernel attributes are set outside any later graph capture
     if (o.fp32)
         for (int l = 1; l <= fine_; ++l) apply<float>(l, w32_.e[l].data(), w32_.tmp[l].data(), st);
@@ -332,8 +335,21 @@ void VelocityMultigrid::apply(int l, const T* x, T* y, cudaStream_t st)
 template <typename T>
 void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st)
 {
-    Work<T>& W  = work<T>();
-    double   ev = lambda_[l];
+    Work<T>& W = work<T>();
+    if (opt_.smoother == 1) {
+        // Jacobi::solve_impl (jacobi.hpp:51-60): x += omega D^-1 (b - A x), one
+        // fused update per step (the first-step form of the Chebyshev kernel)
+        const int64_t n    = W.tmp[l].total();
+        T*            ax   = W.tmp[l].data();
+        T*            d    = W.d[l].data();
+        const T*      invd = W.invdiag[l].data();
+        for (int it = 0; it < opt_.cheb_iters; ++it) {
+            apply<T>(l, x, ax, st);
+            chk(cheb_step<T>(n, x, d, b, ax, invd, static_cast<T>(opt_.jacobi_omega), T(0), true, st), "jacobi");
+        }
+        return;
+    }
+    double ev = lambda_[l];
     if (!std::isfinite(ev) || ev <= 0.0) ev = 1.0;
     const double  lmax = 1.5 * ev, lmin = 0.1 * ev;
     const double  theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);

@@ -51,6 +51,8 @@ struct MgOptions {
     int      gca  = 1;      // 1: Galerkin coarse operators on every coarse level; 0: rediscretised
     bool     fp32 = false;  // FP32 V-cycle (coarsest solve stays FP64)
     uint64_t seed = 12345;  // power-iteration start vectors
+    int      smoother     = 0;    // 0: Chebyshev (cheb_order, cheb_iters), 1: damped Jacobi (cheb_iters steps)
+    double   jacobi_omega = 1.0;  // Jacobi relaxation
 };
 
 // Velocity multigrid (Multigrid, multigrid.hpp:216-432) over levels 0..fine of

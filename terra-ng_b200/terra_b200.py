@@ -27,6 +27,9 @@ _lib = None
 STORED_OFF, STORED_FULL = 0, 1
 
 
+SMOOTHER_CHEBYSHEV, SMOOTHER_JACOBI = 0, 1
+
+
 class SolverOptions(ctypes.Structure):
     """tn_solver_options."""
 
@@ -48,6 +51,8 @@ class SolverOptions(ctypes.Structure):
         ("normalize_pressure", ctypes.c_int),
         ("project_pressure_mean", ctypes.c_int),
         ("cuda_graphs", ctypes.c_int),
+        ("smoother", ctypes.c_int),
+        ("jacobi_omega", ctypes.c_double),
     ]
 
 

@@ -180,6 +180,24 @@ def test_vcycle_matches_oracle(cuda, gca, bcs):
 
 
 @pytest.mark.parametrize("bcs", [(1, 2), (1, 1)])
+def test_vcycle_jacobi_smoother_matches_oracle(cuda, bcs):
+    """One V-cycle with the damped Jacobi smoother (jacobi.hpp:51-60; 3 pre-
+    and post-smoothing steps, omega = 0.8) and a converged coarsest solve,
+    against the oracle at 1e-9."""
+    import torch
+
+    level, nlev = 4, 3
+    sh, k, g, solver, H = _hierarchy(level, nlev, bcs, 1, smoother=T.SMOOTHER_JACOBI, jacobi_omega=0.8,
+                                     chebyshev_iterations=3, coarse_relative_tolerance=1e-13,
+                                     coarse_max_iterations=3000)
+    b = O.enforce_rhs_bcs(sh, consistent(sh, O.seeded_normal(sh.vec_shape, 35)), bcs[0], bcs[1])
+    ref = H.multigrid(smoother="jacobi", omega=0.8).solve(np.zeros(sh.vec_shape), b)
+    x = torch.zeros(sh.vec_shape, dtype=torch.float64, device=cuda)
+    solver.vcycle(x, _t(b))
+    assert rel_err(x.cpu().numpy(), ref) < 1e-9
+
+
+@pytest.mark.parametrize("bcs", [(1, 2), (1, 1)])
 def test_vcycle_reference_coarse_settings(cuda, bcs):
     """The reference's coarsest CG (50 iterations, 1e-6). On the level-2
     coarse problem 50 CG steps reduce the residual by only about 1e-3, and CG

@@ -144,3 +144,14 @@ def test_vjp_logeta_matches_finite_differences(bcs):
         tm[e] -= h
         fd = (J(tp) - J(tm)) / (2 * h)
         assert abs(fd - g[e]) <= 1e-6 * max(abs(g[e]), 1e-3 * np.abs(g).max())
+
+
+def test_oracle_jacobi_smoother():
+    """Damped Jacobi on a diagonal system: x_{k+1} = x_k + omega (b - x_k) / d,
+    so the error shrinks by (1 - omega) per step."""
+    d = np.array([2.0, 4.0, 8.0])
+    b = np.array([1.0, 2.0, 3.0])
+    sol = b / d
+    J = O.Jacobi(1.0 / d, iterations=3, omega=0.5)
+    x = J.solve(lambda v: d * v, np.zeros(3), b)
+    assert np.allclose(x - sol, (0.5 ** 3) * (0.0 - sol))

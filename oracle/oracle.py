@@ -485,6 +485,10 @@ def fgmres(A, x, b, dot, precond, restart, rtol, atol, max_iter, history=None):
         inner = 0
         j = 0
         while j < m and total < max_iter:
+            # each step counts toward max_iter when it starts, so a cycle that
+            # ends early (tolerance met by the estimate only, breakdown) still
+            # lets the loop end (the product's FGMRES counts the same way)
+            total += 1
             z = precond(V[j])
             if not np.all(np.isfinite(z)):
                 z = V[j].copy()
@@ -522,13 +526,11 @@ def fgmres(A, x, b, dot, precond, restart, rtol, atol, max_iter, history=None):
                 history.append(abs_res / init)
             if not np.isfinite(abs_res):
                 inner = j
-                total += 1
                 break
             inner = j + 1
             if abs_res / init <= rtol or abs_res < atol:
                 break
             j += 1
-            total += 1
         y = np.zeros(inner)
         for row in range(inner - 1, -1, -1):
             s = g[row] - sum(H[row, c] * y[c] for c in range(row + 1, inner))

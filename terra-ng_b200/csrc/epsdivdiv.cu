@@ -36,6 +36,7 @@
 #include "tn_wedge_math.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 namespace tn {
@@ -43,6 +44,9 @@ namespace {
 
 // Warps per CTA (tile_y + 1): FP64 needs up to 255 registers per thread (8
 // warps fill the register file), FP32 fits 12 warps.
+// devices a process can drive (per-device launch caches)
+constexpr int kMaxDevices = 64;
+
 template <typename T>
 struct MaxWarps;
 template <>
@@ -600,13 +604,19 @@ int launch_cfg(EddArgs<T> a, int nfields, cudaStream_t st)
         L    = edd_smem_layout<T, CPL>(a.nr, a.ty, a.cx, nfields);
     }
     if (L.total > kSmemLimit) return -5;
-    auto                k = epsdivdiv_kernel<T, CPL, DIAG>;
-    static size_t       configured = 0;
-    if (L.total > configured) {
+    auto k = epsdivdiv_kernel<T, CPL, DIAG>;
+    // the dynamic shared-memory limit is a per-device attribute of the kernel:
+    // raise it once per device (and only upwards)
+    static std::atomic<size_t> configured[kMaxDevices];
+    int                        dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+    if (L.total > configured[dev].load(std::memory_order_relaxed)) {
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total)) !=
             cudaSuccess)
             return -1;
-        configured = L.total;
+        size_t prev = configured[dev].load(std::memory_order_relaxed);
+        while (prev < L.total && !configured[dev].compare_exchange_weak(prev, L.total)) {
+        }
     }
     const int nl = a.nl;
     dim3      grid((nl + a.ty - 1) / a.ty, (nl + a.cx - 1) / a.cx, 10);
@@ -653,11 +663,13 @@ int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream)
         a.cx = p.chunk_x;
     } else {
         // One CTA per SM: pick the x-chunk that minimises waves x steps per CTA.
-        static int sms = 0;
+        static std::atomic<int> sm_count[kMaxDevices];
+        int                     dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+        int sms = sm_count[dev].load(std::memory_order_relaxed);
         if (sms == 0) {
-            int dev = 0;
-            cudaGetDevice(&dev);
             if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+            sm_count[dev].store(sms, std::memory_order_relaxed);
         }
         const int ytiles = (p.nl + a.ty - 1) / a.ty;
         long      best   = -1;

@@ -1028,9 +1028,12 @@ struct PcgConfig {
 int pcg_config(int n, int nc, int nr, int ncls, int nmem, PcgConfig& out)
 {
     static std::mutex                                           mu;
-    static std::map<std::tuple<int, int, int, int, int>, PcgConfig> cache;
-    std::lock_guard<std::mutex>                                 lock(mu);
-    const auto                                                  key = std::make_tuple(n, nc, nr, ncls, nmem);
+    // per device: the function attributes set below belong to the current device
+    static std::map<std::tuple<int, int, int, int, int, int>, PcgConfig> cache;
+    std::lock_guard<std::mutex>                                      lock(mu);
+    int                                                              dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -2;
+    const auto key = std::make_tuple(dev, n, nc, nr, ncls, nmem);
     auto                                                        it  = cache.find(key);
     if (it != cache.end()) {
         out = it->second;

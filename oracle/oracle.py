@@ -191,6 +191,12 @@ class EpsDivDiv:
             lib().tno_epsdivdiv_slow(ctypes.byref(s), _dpp(src), _dpp(dst))
         else:
             lib().tno_epsdivdiv_fast(ctypes.byref(s), _dpp(src), _dpp(dst))
+        if self.bc_cmb == FREESLIP and self.bc_surface == FREESLIP and not s.diagonal:
+            # added to every copy before the interface sum, as the reference does (:711-785)
+            modes = null_space_modes(self.shell)
+            alpha = [PENALTY_EPSILON * self.shell.dot(m, np.stack(src)) for m in modes]
+            for c in range(3):
+                dst[c] += alpha[0] * modes[0][c] + alpha[1] * modes[1][c] + alpha[2] * modes[2][c]
         if comm:
             lib().tno_interface_sum(self.shell.lat_level, self.shell.nr, 3, _dpp(dst))
         return np.stack(dst)
@@ -215,6 +221,41 @@ class EpsDivDiv:
         if rc != 0:
             raise ValueError("vjp needs a per-cell (Q0) coefficient")
         return g
+
+
+PENALTY_EPSILON = 1e-7  # epsilon_divdiv_kerngen.hpp:168
+_MODES_CACHE: dict = {}
+
+
+def null_space_modes(shell: Shell):
+    """Orthonormal rotation modes of the free-slip/free-slip shell (epsilon_divdiv_kerngen.hpp:324-445):
+    e_i x X for the three axes, the normal component removed on both boundaries through the normal-tangential
+    rotation (local_basis_trafo_normal_tangential.hpp:34-76), then modified Gram-Schmidt with owned-node dots."""
+    key = (shell.lat_level, shell.rad_level, shell.r_min, shell.r_max)
+    if key in _MODES_CACHE:
+        return _MODES_CACHE[key]
+    X = shell.physical_coords()
+    modes = []
+    for axis in range(3):
+        a1, a2 = (axis + 1) % 3, (axis + 2) % 3
+        m = np.zeros(shell.vec_shape)
+        m[a1] = X[..., a2]
+        m[a2] = -X[..., a1]
+        for r in (0, shell.nr - 1):
+            for d in range(10):
+                for x in range(shell.nl):
+                    for y in range(shell.nl):
+                        Rm = trafo_nt(shell.coords[d, x, y])
+                        nt = Rm @ m[:, d, x, y, r]
+                        nt[0] = 0.0
+                        m[:, d, x, y, r] = Rm.T @ nt
+        modes.append(m)
+    for i in range(3):
+        for j in range(i):
+            modes[i] = modes[i] - shell.dot(modes[i], modes[j]) * modes[j]
+        modes[i] = modes[i] * (1.0 / math.sqrt(shell.dot(modes[i], modes[i])))
+    _MODES_CACHE[key] = modes
+    return modes
 
 
 def gca_coarsen(fine_op: EpsDivDiv, fine_mats=None):
@@ -328,6 +369,56 @@ def enforce_rhs_bcs(shell: Shell, f, bc_cmb, bc_surface):
             un = np.einsum("cdxy,dxyc->dxy", f[:, :, :, :, r], n) / np.sum(n * n, axis=-1)
             f[:, :, :, :, r] -= np.moveaxis(un[..., None] * n, -1, 0)
     return f
+
+
+INNER_FLAG, BOUNDARY_FLAG, CMB_FLAG, SURFACE_FLAG = 1, 2, 6, 10  # grid/shell/bit_masks.hpp:11-19
+
+
+def has_flag(mask, flag):
+    """util/bit_masking.hpp:43-53: all bits of flag set; NO_FLAG matches only unflagged nodes."""
+    mask = np.asarray(mask)
+    if flag == 0:
+        return mask == 0
+    return (mask & flag) == flag
+
+
+def shell_boundary_flag(bc_cmb, bc_surface, bcf):
+    """get_shell_boundary_flag (grid/shell/bit_masks.hpp:68-77): the FIRST boundary carrying condition bcf
+    (CMB before SURFACE), or NO_FLAG."""
+    for sbf, bc in ((CMB_FLAG, bc_cmb), (SURFACE_FLAG, bc_surface)):
+        if bc == bcf:
+            return sbf
+    return 0
+
+
+def assign_masked(shell: Shell, f, flag, value=0.0):
+    """assign_masked_else_keep_old on every component (kernels/common/grid_operations.hpp:54-101)."""
+    f = np.array(f, dtype=np.float64, copy=True)
+    m = has_flag(shell.boundary_mask, flag)
+    f[:, m] = value
+    return f
+
+
+def freeslip_project(shell: Shell, f, flag):
+    """strong_algebraic_freeslip_enforcement_in_place (strong_algebraic_freeslip_enforcement.hpp:22-38): at
+    nodes carrying flag, rotate to (n, t1, t2), zero the normal part, rotate back."""
+    f = np.array(f, dtype=np.float64, copy=True)
+    idx = np.argwhere(has_flag(shell.boundary_mask, flag))
+    for d, x, y, r in idx:
+        Rm = trafo_nt(shell.coords[d, x, y])
+        nt = Rm @ f[:, d, x, y, r]
+        nt[0] = 0.0
+        f[:, d, x, y, r] = Rm.T @ nt
+    return f
+
+
+def rhs_enforce_app(shell: Shell, f, bc_cmb, bc_surface):
+    """The application's right-hand-side treatment (stokes_solver.hpp:662-671): zero the velocity on the
+    boundary get_shell_boundary_flag returns for DIRICHLET, then remove the normal component on the one it
+    returns for FREESLIP. With Dirichlet on both boundaries only the CMB is zeroed (the lookup stops at the
+    first match)."""
+    f = assign_masked(shell, f, shell_boundary_flag(bc_cmb, bc_surface, DIRICHLET))
+    return freeslip_project(shell, f, shell_boundary_flag(bc_cmb, bc_surface, FREESLIP))
 
 
 # --------------------------------------------------------------------------

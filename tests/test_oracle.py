@@ -35,7 +35,11 @@ def test_operator_symmetric(bcs):
     u = consistent(sh, O.seeded_normal(sh.vec_shape, 4))
     v = consistent(sh, O.seeded_normal(sh.vec_shape, 5))
     a, b = sh.dot(v, op.apply(u)), sh.dot(u, op.apply(v))
-    assert abs(a - b) <= 1e-12 * abs(a)
+    # free-slip on both boundaries: the reference adds its 1e-7 rotation penalty on every interface copy
+    # before the interface sum (epsilon_divdiv_kerngen.hpp:711-791), so duplicated nodes carry it times
+    # their multiplicity and exact symmetry holds only up to the penalty's size
+    tol = 1e-8 if bcs == (2, 2) else 1e-12
+    assert abs(a - b) <= tol * abs(a)
 
 
 def test_rigid_motions_in_neumann_kernel():

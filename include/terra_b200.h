@@ -121,7 +121,13 @@ int tn_operator_components(const tn_operator* op, int* src_components, int* dst_
 int tn_operator_set_modes(tn_operator* op, int apply_mode, int comm_mode);
 /* set_diagonal (epsilon_divdiv_kerngen.hpp:455) */
 int tn_operator_set_diagonal(tn_operator* op, int diagonal);
-/* set_boundary_conditions (epsilon_divdiv_kerngen.hpp:474-481) */
+/* set_boundary_conditions (epsilon_divdiv_kerngen.hpp:474-481). With free slip
+ * on both boundaries an epsilon-div-div operator adds the reference's null-space
+ * penalty dst += 1e-7 sum_i (n_i^T src)_owned n_i over the three orthonormal
+ * rotation modes n_i, on every interface copy before the interface sum and not
+ * in diagonal mode (init_penalty and apply_impl, epsilon_divdiv_kerngen.hpp:
+ * 324-445, :711-785); the modes are built by the first apply or this call
+ * (synchronous, before any stream capture). */
 int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surface);
 /* Override the CTA tile (0 = default); for tuning. */
 int tn_operator_set_tile(tn_operator* op, int tile_y, int chunk_x);
@@ -195,6 +201,63 @@ int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void*
  * randomize (grid_operations.hpp:748-773), whose stream depends on the backend. */
 int tn_vec_random(tn_shell* shell, int level, int precision, int ncomp, uint64_t seed, void* const* comps_dev,
                   void* stream);
+
+/* Remaining VectorLike operations (src/terra/linalg/vector.hpp:8-42; kernels in
+ * src/terra/kernels/common/grid_operations.hpp). Entry-wise over all stored
+ * nodes of ncomp (1..4) components of one level.
+ *   invert_entries       y = 1 / y                     (grid_operations.hpp:232-253)
+ *   scale_with_vector    y = y .* x                    (mult_elementwise_inplace, :255-273)
+ *   max_abs_entry        max |a| over all entries      (:315-330); synchronous on `stream`
+ *   has_nan_or_inf       1 if any entry is NaN or Inf  (:331-346); synchronous on `stream`
+ *   swap                 a <-> b, entry-wise           (vector_q1.hpp swap_impl) */
+int tn_vec_invert(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, void* stream);
+int tn_vec_scale(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, const void* const* x_dev,
+                 void* stream);
+int tn_vec_max_abs(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev, double* result,
+                   void* stream);
+int tn_vec_has_nan_or_inf(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev, int* result,
+                          void* stream);
+int tn_vec_swap(tn_shell* shell, int level, int precision, int ncomp, void* const* a_dev, void* const* b_dev,
+                void* stream);
+/* Precision casts of n entries (the FP64 <-> FP32 boundary of the mixed-precision
+ * solve; no counterpart in the FP64-only reference): direction TN_F64 means
+ * FP64 in -> FP32 out, TN_F32 means FP32 in -> FP64 out. */
+int tn_vec_cast(int64_t n, int direction, const void* in_dev, void* out_dev, void* stream);
+
+/* ---- boundary treatment of right-hand sides --------------------------------
+ * Node flags are the ShellBoundaryFlag values (src/terra/grid/shell/bit_masks.hpp:
+ * 11-19): TN_FLAG_CMB on r = 0, TN_FLAG_SURFACE on r = nr-1, TN_FLAG_INNER else;
+ * a node matches `flag` when it carries all of its bits (util/bit_masking.hpp:
+ * 43-53; flag 0 matches no node of a shell). */
+#define TN_FLAG_INNER 1
+#define TN_FLAG_BOUNDARY 2
+#define TN_FLAG_CMB 6
+#define TN_FLAG_SURFACE 10
+/* v = value on matching nodes, every component (assign_masked_else_keep_old,
+ * src/terra/kernels/common/grid_operations.hpp:54-131; with value 0 the strong
+ * Dirichlet step strong_algebraic_homogeneous_velocity_dirichlet_enforcement_
+ * stokes_like, src/terra/fe/strong_algebraic_dirichlet_enforcement.hpp:114-123). */
+int tn_vec_assign_masked(tn_shell* shell, int level, int precision, int ncomp, void* const* v_dev, int flag,
+                         double value, void* stream);
+/* On matching nodes of a 3-component vector: direction 0 rotates Cartesian
+ * components into (normal, tangent 1, tangent 2), 1 rotates back
+ * (cartesian_to_normal_tangential_in_place / normal_tangential_to_cartesian_in_place,
+ * src/terra/linalg/trafo/local_basis_trafo_normal_tangential.hpp:34-186). */
+int tn_vec_rotate_normal_tangential(tn_shell* shell, int level, int precision, void* const* v_dev, int flag,
+                                    int direction, void* stream);
+/* Remove the normal component on matching nodes (rotate, zero, rotate back:
+ * strong_algebraic_freeslip_enforcement_in_place,
+ * src/terra/fe/strong_algebraic_freeslip_enforcement.hpp:22-38). */
+int tn_vec_freeslip_project(tn_shell* shell, int level, int precision, void* const* v_dev, int flag, void* stream);
+/* The application's right-hand-side treatment (apps/mantlecirculation/src/
+ * stokes_solver.hpp:662-671): the Dirichlet step on the boundary
+ * get_shell_boundary_flag(bcs, DIRICHLET) returns, then the free-slip projection
+ * on the one it returns for FREESLIP (src/terra/grid/shell/bit_masks.hpp:68-77:
+ * the first match, CMB before SURFACE, so with Dirichlet on both boundaries only
+ * the CMB rows are zeroed, as in the reference). u_dev: the 3 velocity
+ * components of a right-hand side on `level`. */
+int tn_stokes_rhs_enforce(tn_shell* shell, int level, int precision, int bc_cmb, int bc_surface, void* const* u_dev,
+                          void* stream);
 
 /* ---- stored element matrices and Galerkin coarse operators -----------------
  * set_stored_matrix_mode (epsilon_divdiv_kerngen.hpp:483-528) with

@@ -229,8 +229,9 @@ _MODES_CACHE: dict = {}
 
 def null_space_modes(shell: Shell):
     """Orthonormal rotation modes of the free-slip/free-slip shell (epsilon_divdiv_kerngen.hpp:324-445):
-    e_i x X for the three axes, the normal component removed on both boundaries through the normal-tangential
-    rotation (local_basis_trafo_normal_tangential.hpp:34-76), then modified Gram-Schmidt with owned-node dots."""
+    e_i x X for the three axes, then modified Gram-Schmidt with owned-node dots. The reference also runs a
+    free-slip pass over the modes, but on nodes flagged CMB | SURFACE together, which no node is, so it leaves
+    them unchanged (the rotation modes are tangential on every sphere anyway)."""
     key = (shell.lat_level, shell.rad_level, shell.r_min, shell.r_max)
     if key in _MODES_CACHE:
         return _MODES_CACHE[key]
@@ -241,14 +242,6 @@ def null_space_modes(shell: Shell):
         m = np.zeros(shell.vec_shape)
         m[a1] = X[..., a2]
         m[a2] = -X[..., a1]
-        for r in (0, shell.nr - 1):
-            for d in range(10):
-                for x in range(shell.nl):
-                    for y in range(shell.nl):
-                        Rm = trafo_nt(shell.coords[d, x, y])
-                        nt = Rm @ m[:, d, x, y, r]
-                        nt[0] = 0.0
-                        m[:, d, x, y, r] = Rm.T @ nt
         modes.append(m)
     for i in range(3):
         for j in range(i):

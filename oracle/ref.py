@@ -67,8 +67,12 @@ def lib(threads: int = 0):
         L.tnr_prolongate_add.argtypes = [I, D, D, dp, dp]
         L.tnr_restrict.argtypes = [I, D, D, dp, dp]
         L.tnr_gca.argtypes = [I, I, D, D, dp, dp]
-        L.tnr_stokes_fgmres.argtypes = [I, I, D, D, I, I, dp, dpp, dp, dpp, I, I, D, D, I, I, I, I, I, dp, dp, dp,
-                                        I, ctypes.POINTER(I)]
+        L.tnr_stokes_create.argtypes = [I, I, D, D, I, I, dp, dpp, dp, dpp, I, I, I, I, I, I,
+                                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(D)]
+        L.tnr_stokes_solve.argtypes = [ctypes.c_void_p, D, D, I, dp, dp, dp, I, ctypes.POINTER(I), ctypes.POINTER(D)]
+        L.tnr_stokes_destroy.argtypes = [ctypes.c_void_p]
+        L.tnr_stokes_destroy.restype = None
+        L.tnr_epsdivdiv_time.argtypes = [I, D, D, dp, I, I, dp, I, dp]
         L.tnr_rhs_enforce.argtypes = [I, D, D, I, I, dp]
         _check(L, L.tnr_init(int(threads) if threads > 0 else (os.cpu_count() or 1)))
         _lib = L
@@ -193,27 +197,68 @@ def rhs_enforce(lat, f, bc_cmb, bc_surface, r_min=0.55, r_max=1.0):
     return out
 
 
+class StokesRef:
+    """The reference application's Stokes solver (FGMRES + block-triangular GMG), built once."""
+
+    def __init__(self, lat, num_levels, k, k_schur, k_levels=None, start=None, bc_cmb=DIRICHLET, bc_surface=FREESLIP,
+                 gca=True, restart=30, cheb_order=2, cheb_iterations=2, power_iterations=10, vcycles=1, r_min=0.55,
+                 r_max=1.0):
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._keep = []
+
+        def arr(lst):
+            if lst is None:
+                return None
+            cs = [None if a is None else _c(a) for a in lst]
+            self._keep.append(cs)
+            return (dp * len(cs))(*[_dp(a) if a is not None else None for a in cs])
+
+        k, k_schur = _c(k), _c(k_schur)
+        self._keep.append((k, k_schur))
+        h, t = ctypes.c_void_p(), ctypes.c_double()
+        L = lib()
+        _check(L, L.tnr_stokes_create(lat, num_levels, r_min, r_max, bc_cmb, bc_surface, _dp(k), arr(k_levels),
+                                      _dp(k_schur), arr(start), int(gca), restart, cheb_order, cheb_iterations,
+                                      power_iterations, vcycles, ctypes.byref(h), ctypes.byref(t)))
+        self._h, self.setup_seconds = h, t.value
+
+    def solve(self, b, x0=None, rtol=1e-8, atol=1e-30, max_it=100):
+        """Returns (x, relative residual history, wall seconds of the solve)."""
+        b = _c(b)
+        x = np.zeros_like(b) if x0 is None else _c(x0).copy()
+        hist = np.zeros(max_it + 64)
+        n, t = ctypes.c_int(0), ctypes.c_double()
+        L = lib()
+        _check(L, L.tnr_stokes_solve(self._h, rtol, atol, max_it, _dp(b), _dp(x), _dp(hist), len(hist),
+                                     ctypes.byref(n), ctypes.byref(t)))
+        return x, hist[: n.value].copy(), t.value
+
+    def close(self):
+        if self._h:
+            lib().tnr_stokes_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tnr_stokes_destroy(self._h)
+            self._h = None
+
+
 def stokes_fgmres(lat, num_levels, k, k_schur, b, x0=None, k_levels=None, start=None, bc_cmb=DIRICHLET,
                   bc_surface=FREESLIP, gca=True, restart=30, rtol=1e-8, atol=1e-30, max_it=100, cheb_order=2,
                   cheb_iterations=2, power_iterations=10, vcycles=1, r_min=0.55, r_max=1.0):
     """The reference application's Stokes solve; returns (x, relative residual history)."""
-    b = _c(b)
-    x = np.zeros_like(b) if x0 is None else _c(x0).copy()
-    dp = ctypes.POINTER(ctypes.c_double)
-    keep = []
+    S = StokesRef(lat, num_levels, k, k_schur, k_levels=k_levels, start=start, bc_cmb=bc_cmb, bc_surface=bc_surface,
+                  gca=gca, restart=restart, cheb_order=cheb_order, cheb_iterations=cheb_iterations,
+                  power_iterations=power_iterations, vcycles=vcycles, r_min=r_min, r_max=r_max)
+    x, hist, _ = S.solve(b, x0=x0, rtol=rtol, atol=atol, max_it=max_it)
+    S.close()
+    return x, hist
 
-    def arr(lst):
-        if lst is None:
-            return None
-        cs = [None if a is None else _c(a) for a in lst]
-        keep.append(cs)
-        return (dp * len(cs))(*[_dp(a) if a is not None else None for a in cs])
 
-    hist = np.zeros(max_it + 64)
-    n = ctypes.c_int(0)
+def epsdivdiv_time(lat, k, src, reps=5, bc_cmb=DIRICHLET, bc_surface=FREESLIP, r_min=0.55, r_max=1.0):
+    """Seconds of each of `reps` reference applies after one warm-up (fast path, with the interface sum)."""
+    out = np.zeros(reps)
     L = lib()
-    _check(L, L.tnr_stokes_fgmres(lat, num_levels, r_min, r_max, bc_cmb, bc_surface, _dp(_c(k)), arr(k_levels),
-                                  _dp(_c(k_schur)), arr(start), int(gca), restart, rtol, atol, max_it, cheb_order,
-                                  cheb_iterations, power_iterations, vcycles, _dp(b), _dp(x), _dp(hist),
-                                  len(hist), ctypes.byref(n)))
-    return x, hist[: n.value].copy()
+    _check(L, L.tnr_epsdivdiv_time(lat, r_min, r_max, _dp(_c(k)), bc_cmb, bc_surface, _dp(_c(src)), reps, _dp(out)))
+    return out

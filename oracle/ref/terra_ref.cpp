@@ -14,8 +14,10 @@
 
 #include <Kokkos_Core.hpp>
 
+#include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <iostream>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -210,20 +212,31 @@ void guard_small_teams( G& gradient )
         gradient.force_slow_path();
 }
 
+// The reference logs its set-up to std::cout (util/logging.hpp); inside a call the stream is pointed at a
+// sink so that a host process printing machine-readable lines keeps a clean stdout.
+struct NullBuf : std::streambuf
+{
+    int overflow( int c ) override { return c == EOF ? 0 : c; }
+};
+
 template < typename F >
 int guarded( F&& f )
 {
+    static NullBuf  sink;
+    std::streambuf* saved = std::cout.rdbuf( &sink );
+    int             rc    = 0;
     try
     {
         f();
         Kokkos::fence();
-        return 0;
     }
     catch ( const std::exception& e )
     {
         g_error = e.what();
-        return -1;
+        rc      = -1;
     }
+    std::cout.rdbuf( saved );
+    return rc;
 }
 
 using Viscous  = fe::wedge::operators::shell::EpsilonDivDivKerngen< double >;
@@ -473,141 +486,181 @@ int tnr_gca( int fine_lat, int coarse_lat, double r_min, double r_max, const dou
 /// with Chebyshev(order, iterations, power_iterations) smoothing on levels lat-num_levels+1 .. lat, GCA coarse
 /// operators when gca != 0 (else the coarse operators take k_levels), PCG(50, 1e-6, 1e-16) on the coarsest
 /// level; Schur block = inverse lumped KMass with coefficient k_schur (pressure level). start[l] (optional,
-/// coarsest first) are the power-iteration start vectors, 3 components each. b and x are Stokes vectors: 3
-/// velocity components on level lat, then pressure on level lat-1. x is the initial guess on entry.
-/// history receives the relative residual after each iteration (history[0] = 1); *n_hist its length.
-int tnr_stokes_fgmres( int lat, int num_levels, double r_min, double r_max, int bc_cmb, int bc_surface,
+/// coarsest first) are the power-iteration start vectors, 3 components each; the smoothers estimate their
+/// spectra on the first solve. tnr_stokes_create builds everything (*setup_seconds: its wall time);
+/// tnr_stokes_solve runs FGMRES on b from the initial guess in x (b and x: 3 velocity components on level lat,
+/// then pressure on level lat-1), fills history with the relative residual per iteration (history[0] = 1) and
+/// *seconds with the wall time of the solve alone.
+struct StokesRef
+{
+    using Smoother   = linalg::solvers::Chebyshev< Viscous >;
+    using Coarse     = linalg::solvers::PCG< Viscous >;
+    using MG         = linalg::solvers::Multigrid< Viscous, Prolong, Restrict, Smoother, Coarse >;
+    using Schur      = linalg::solvers::DiagonalSolver< PMass >;
+    using PrecStokes = linalg::solvers::BlockTriangularPreconditioner2x2< Stokes, Viscous, PMass, Grad, MG, Schur >;
+
+    std::vector< Level* >                         lv;
+    std::map< long, std::vector< double > >       starts;
+    std::shared_ptr< util::Table >                table;
+    std::unique_ptr< Stokes >                     K, K_neumann;
+    std::vector< Viscous >                        A_c;
+    std::vector< Prolong >                        Pv;
+    std::vector< Restrict >                       Rv;
+    std::vector< VectorQ1Vec< double > >          inv_diag, tmp, tmp2, tmp_r, tmp_e, coarse_tmps;
+    std::unique_ptr< Coarse >                     coarse;
+    std::unique_ptr< MG >                         mg;
+    std::unique_ptr< PMass >                      pmass;
+    VectorQ1Scalar< double >                      lumped;
+    std::unique_ptr< Schur >                      schur;
+    VectorQ1IsoQ2Q1< double >                     prec_tmp;
+    std::unique_ptr< PrecStokes >                 prec;
+    std::vector< VectorQ1IsoQ2Q1< double > >      ftmp;
+    VectorQ1IsoQ2Q1< double >                     xv, bv;
+    int                                           restart = 30;
+};
+
+int tnr_stokes_create( int lat, int num_levels, double r_min, double r_max, int bc_cmb, int bc_surface,
                        const double* k, const double* const* k_levels, const double* k_schur,
-                       const double* const* start, int gca, int restart, double rtol, double atol, int max_it,
-                       int cheb_order, int cheb_iterations, int power_iterations, int vcycles, const double* b,
-                       double* x, double* history, int max_hist, int* n_hist )
+                       const double* const* start, int gca, int restart, int cheb_order, int cheb_iterations,
+                       int power_iterations, int vcycles, void** out, double* setup_seconds )
 {
     return guarded( [&] {
-        const int coarsest = lat - num_levels + 1;
+        const auto t0       = std::chrono::steady_clock::now();
+        const int  coarsest = lat - num_levels + 1;
         if ( coarsest < 0 || num_levels < 2 )
             throw std::runtime_error( "bad level range" );
-        std::vector< Level* > lv;
+        auto S = std::make_unique< StokesRef >();
         for ( int l = coarsest; l <= lat; ++l )
-            lv.push_back( &level( l, l, r_min, r_max ) );
-        Level&             F = *lv.back();
-        Level&             P = *lv[num_levels - 2];
+            S->lv.push_back( &level( l, l, r_min, r_max ) );
+        Level&             F = *S->lv.back();
+        Level&             P = *S->lv[num_levels - 2];
         BoundaryConditions bcs, neumann;
         set_bcs( bcs, bc_cmb, bc_surface );
         set_bcs( neumann, 0, 0 );
-
-        tnr::start_vectors().by_size.clear();
         if ( start )
             for ( int l = 0; l < num_levels; ++l )
                 if ( start[l] )
-                    tnr::start_vectors().by_size[10L * lv[l]->nl * lv[l]->nl * lv[l]->nr] = start[l];
+                {
+                    const long n = 10L * S->lv[l]->nl * S->lv[l]->nl * S->lv[l]->nr;
+                    S->starts[n].assign( start[l], start[l] + 3 * n );
+                }
 
-        auto  table = std::make_shared< util::Table >();
-        auto  kf    = scalar_field( F, k, "eta" );
-        Stokes K( *F.domain, *P.domain, F.coords, F.radii, F.boundary, kf, bcs, false );
-        Stokes K_neumann( *F.domain, *P.domain, F.coords, F.radii, F.boundary, kf, neumann, false );
-        guard_small_teams( K.block_12() );
+        S->table     = std::make_shared< util::Table >();
+        auto kf      = scalar_field( F, k, "eta" );
+        S->K         = std::make_unique< Stokes >( *F.domain, *P.domain, F.coords, F.radii, F.boundary, kf, bcs, false );
+        S->K_neumann = std::make_unique< Stokes >( *F.domain, *P.domain, F.coords, F.radii, F.boundary, kf, neumann,
+                                                   false );
+        guard_small_teams( S->K->block_12() );
 
-        Level&                   L0 = *lv[0];
+        Level&                   L0 = *S->lv[0];
         VectorQ1Scalar< double > elements( "GCAElements", *L0.domain, L0.owned );
         linalg::assign( elements, gca ? 1.0 : 0.0 );
-
-        std::vector< Viscous >  A_c;
-        std::vector< Prolong >  Pv;
-        std::vector< Restrict > Rv;
         for ( int l = 0; l < num_levels - 1; ++l )
         {
-            Level& L = *lv[l];
-            A_c.emplace_back( *L.domain, L.coords, L.radii, L.boundary,
-                              scalar_field( L, k_levels ? k_levels[l] : nullptr, "k_c" ), bcs, false );
+            Level& L = *S->lv[l];
+            S->A_c.emplace_back( *L.domain, L.coords, L.radii, L.boundary,
+                                 scalar_field( L, k_levels ? k_levels[l] : nullptr, "k_c" ), bcs, false );
             if ( gca )
-                A_c.back().set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, l, elements.grid_data() );
-            Pv.emplace_back( linalg::OperatorApplyMode::Add );
-            Rv.emplace_back( *L.domain );
+                S->A_c.back().set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, l,
+                                                      elements.grid_data() );
+            S->Pv.emplace_back( linalg::OperatorApplyMode::Add );
+            S->Rv.emplace_back( *L.domain );
         }
         if ( gca )
             for ( int l = num_levels - 2; l >= 0; --l )
                 linalg::solvers::TwoGridGCA< double, Viscous >(
-                    l == num_levels - 2 ? K_neumann.block_11() : A_c[l + 1], A_c[l], l, elements.grid_data() );
+                    l == num_levels - 2 ? S->K_neumann->block_11() : S->A_c[l + 1], S->A_c[l], l,
+                    elements.grid_data() );
 
-        std::vector< VectorQ1Vec< double > > inv_diag, tmp, tmp2, tmp_r, tmp_e;
         for ( int l = 0; l < num_levels; ++l )
         {
-            Level& L = *lv[l];
-            tmp.emplace_back( "tmp_mg", *L.domain, L.owned );
-            tmp2.emplace_back( "tmp_mg_2", *L.domain, L.owned );
+            Level& L = *S->lv[l];
+            S->tmp.emplace_back( "tmp_mg", *L.domain, L.owned );
+            S->tmp2.emplace_back( "tmp_mg_2", *L.domain, L.owned );
             if ( l < num_levels - 1 )
             {
-                tmp_r.emplace_back( "tmp_mg_r", *L.domain, L.owned );
-                tmp_e.emplace_back( "tmp_mg_e", *L.domain, L.owned );
+                S->tmp_r.emplace_back( "tmp_mg_r", *L.domain, L.owned );
+                S->tmp_e.emplace_back( "tmp_mg_e", *L.domain, L.owned );
             }
-            inv_diag.emplace_back( "inverse_diagonal", *L.domain, L.owned );
+            S->inv_diag.emplace_back( "inverse_diagonal", *L.domain, L.owned );
             VectorQ1Vec< double > ones( "ones", *L.domain, L.owned );
             linalg::assign( ones, 1.0 );
-            auto& A = ( l == num_levels - 1 ) ? K.block_11() : A_c[l];
+            auto& A = ( l == num_levels - 1 ) ? S->K->block_11() : S->A_c[l];
             A.set_diagonal( true );
-            linalg::apply( A, ones, inv_diag.back() );
+            linalg::apply( A, ones, S->inv_diag.back() );
             A.set_diagonal( false );
-            linalg::invert_entries( inv_diag.back() );
+            linalg::invert_entries( S->inv_diag.back() );
         }
 
-        using Smoother = linalg::solvers::Chebyshev< Viscous >;
-        using Coarse   = linalg::solvers::PCG< Viscous >;
-        using MG       = linalg::solvers::Multigrid< Viscous, Prolong, Restrict, Smoother, Coarse >;
-        std::vector< Smoother > smoothers;
+        std::vector< StokesRef::Smoother > smoothers;
         for ( int l = 0; l < num_levels; ++l )
-            smoothers.emplace_back( cheb_order, inv_diag[l], std::vector< VectorQ1Vec< double > >{ tmp[l], tmp2[l] },
-                                    cheb_iterations, power_iterations );
-        std::vector< VectorQ1Vec< double > > coarse_tmps;
+            smoothers.emplace_back( cheb_order, S->inv_diag[l],
+                                    std::vector< VectorQ1Vec< double > >{ S->tmp[l], S->tmp2[l] }, cheb_iterations,
+                                    power_iterations );
         for ( int i = 0; i < 4; ++i )
-            coarse_tmps.emplace_back( "tmp_coarse_grid", *L0.domain, L0.owned );
-        Coarse coarse( linalg::solvers::IterativeSolverParameters{ 50, 1e-6, 1e-16 }, table, coarse_tmps );
-        coarse.set_tag( "coarse_grid_pcg" );
-        MG mg( Pv, Rv, A_c, tmp_r, tmp_e, tmp, smoothers, smoothers, coarse, vcycles, 1e-6 );
+            S->coarse_tmps.emplace_back( "tmp_coarse_grid", *L0.domain, L0.owned );
+        S->coarse = std::make_unique< StokesRef::Coarse >(
+            linalg::solvers::IterativeSolverParameters{ 50, 1e-6, 1e-16 }, S->table, S->coarse_tmps );
+        S->coarse->set_tag( "coarse_grid_pcg" );
+        S->mg = std::make_unique< StokesRef::MG >( S->Pv, S->Rv, S->A_c, S->tmp_r, S->tmp_e, S->tmp, smoothers,
+                                                   smoothers, *S->coarse, vcycles, 1e-6 );
 
         VectorQ1Scalar< double > kp( "k_pm", *P.domain, P.owned );
         load( kp.grid_data(), k_schur );
-        PMass pmass( *P.domain, P.coords, P.radii, kp.grid_data(), false );
-        pmass.set_lumped_diagonal( true );
-        VectorQ1Scalar< double > lumped( "lumped_diagonal_pmass", *P.domain, P.owned );
+        S->pmass = std::make_unique< PMass >( *P.domain, P.coords, P.radii, kp.grid_data(), false );
+        S->pmass->set_lumped_diagonal( true );
+        S->lumped = VectorQ1Scalar< double >( "lumped_diagonal_pmass", *P.domain, P.owned );
         {
             VectorQ1Scalar< double > ones( "ones", *P.domain, P.owned );
             linalg::assign( ones, 1.0 );
-            linalg::apply( pmass, ones, lumped );
+            linalg::apply( *S->pmass, ones, S->lumped );
         }
-        linalg::solvers::DiagonalSolver< PMass > schur( lumped );
-
-        VectorQ1IsoQ2Q1< double > prec_tmp( "triangular_prec_tmp", *F.domain, *P.domain, F.owned, P.owned );
-        using PrecStokes =
-            linalg::solvers::BlockTriangularPreconditioner2x2< Stokes, Viscous, PMass, Grad, MG,
-                                                               linalg::solvers::DiagonalSolver< PMass > >;
-        PrecStokes prec( K.block_11(), pmass, K.block_12(), prec_tmp, mg, schur );
-
-        std::vector< VectorQ1IsoQ2Q1< double > > ftmp;
+        S->schur    = std::make_unique< StokesRef::Schur >( S->lumped );
+        S->prec_tmp = VectorQ1IsoQ2Q1< double >( "triangular_prec_tmp", *F.domain, *P.domain, F.owned, P.owned );
+        S->prec     = std::make_unique< StokesRef::PrecStokes >( S->K->block_11(), *S->pmass, S->K->block_12(),
+                                                             S->prec_tmp, *S->mg, *S->schur );
         for ( int i = 0; i < 2 * restart + 4; ++i )
-            ftmp.emplace_back( "stokes_tmp_fgmres", *F.domain, *P.domain, F.owned, P.owned );
-        linalg::solvers::FGMRES< Stokes, PrecStokes > fgmres(
-            ftmp,
-            linalg::solvers::FGMRESOptions< double >{ .restart                     = restart,
+            S->ftmp.emplace_back( "stokes_tmp_fgmres", *F.domain, *P.domain, F.owned, P.owned );
+        S->xv      = VectorQ1IsoQ2Q1< double >( "u", *F.domain, *P.domain, F.owned, P.owned );
+        S->bv      = VectorQ1IsoQ2Q1< double >( "f", *F.domain, *P.domain, F.owned, P.owned );
+        S->restart = restart;
+        Kokkos::fence();
+        *setup_seconds = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+        *out           = S.release();
+    } );
+}
+
+int tnr_stokes_solve( void* h, double rtol, double atol, int max_it, const double* b, double* x, double* history,
+                      int max_hist, int* n_hist, double* seconds )
+{
+    return guarded( [&] {
+        auto*      S  = static_cast< StokesRef* >( h );
+        const long nu = S->lv.back()->nodes();
+        tnr::start_vectors().by_size.clear();
+        for ( const auto& [n, v] : S->starts )
+            tnr::start_vectors().by_size[n] = v.data();
+        linalg::solvers::FGMRES< Stokes, StokesRef::PrecStokes > fgmres(
+            S->ftmp,
+            linalg::solvers::FGMRESOptions< double >{ .restart                     = S->restart,
                                                       .relative_residual_tolerance = rtol,
                                                       .absolute_residual_tolerance = atol,
                                                       .max_iterations              = max_it },
-            table, prec );
+            S->table, *S->prec );
         fgmres.set_tag( "stokes_fgmres" );
-
-        VectorQ1IsoQ2Q1< double > xv( "u", *F.domain, *P.domain, F.owned, P.owned );
-        VectorQ1IsoQ2Q1< double > bv( "f", *F.domain, *P.domain, F.owned, P.owned );
-        const long                nu = F.nodes();
-        load( xv.block_1().grid_data(), x );
-        load( xv.block_2().grid_data(), x + 3 * nu );
-        load( bv.block_1().grid_data(), b );
-        load( bv.block_2().grid_data(), b + 3 * nu );
-        linalg::solvers::solve( fgmres, K, xv, bv );
+        S->table->clear();
+        load( S->xv.block_1().grid_data(), x );
+        load( S->xv.block_2().grid_data(), x + 3 * nu );
+        load( S->bv.block_1().grid_data(), b );
+        load( S->bv.block_2().grid_data(), b + 3 * nu );
         Kokkos::fence();
-        store( xv.block_1().grid_data(), x );
-        store( xv.block_2().grid_data(), x + 3 * nu );
-
+        const auto t0 = std::chrono::steady_clock::now();
+        linalg::solvers::solve( fgmres, *S->K, S->xv, S->bv );
+        Kokkos::fence();
+        *seconds = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+        store( S->xv.block_1().grid_data(), x );
+        store( S->xv.block_2().grid_data(), x + 3 * nu );
         int n = 0;
-        for ( const auto& row : table->rows() )
+        for ( const auto& row : S->table->rows() )
         {
             const auto tag = row.find( "tag" );
             if ( tag == row.end() || util::Table::value_to_string( tag->second ) != "stokes_fgmres" )
@@ -618,6 +671,37 @@ int tnr_stokes_fgmres( int lat, int num_levels, double r_min, double r_max, int 
         }
         *n_hist = n;
         tnr::start_vectors().by_size.clear();
+    } );
+}
+
+void tnr_stokes_destroy( void* h )
+{
+    delete static_cast< StokesRef* >( h );
+}
+
+/// Wall time of `reps` consecutive EpsilonDivDivKerngen<double> applies (Replace + CommunicateAdditively, fast
+/// path chosen by the boundary conditions) after one warm-up apply, as the reference's operator benchmark
+/// times them (apps/benchmarks/performance/benchmark_operators.cpp): seconds[i] per apply.
+int tnr_epsdivdiv_time( int lat, double r_min, double r_max, const double* k, int bc_cmb, int bc_surface,
+                        const double* src, int reps, double* seconds )
+{
+    return guarded( [&] {
+        Level&             L  = level( lat, lat, r_min, r_max );
+        auto               kk = scalar_field( L, k, "k" );
+        BoundaryConditions bcs;
+        set_bcs( bcs, bc_cmb, bc_surface );
+        Viscous               A( *L.domain, L.coords, L.radii, L.boundary, kk, bcs, false );
+        VectorQ1Vec< double > s( "src", *L.domain, L.owned ), d( "dst", *L.domain, L.owned );
+        load( s.grid_data(), src );
+        linalg::apply( A, s, d );
+        Kokkos::fence();
+        for ( int i = 0; i < reps; ++i )
+        {
+            const auto t0 = std::chrono::steady_clock::now();
+            linalg::apply( A, s, d );
+            Kokkos::fence();
+            seconds[i] = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+        }
     } );
 }
 

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/terra_b200.h"
+#include "tn_boundary.hpp"
 #include "tn_solver.hpp"
 
 struct tn_shell {
@@ -146,6 +147,68 @@ tn::EpsDivDivOp* as_edd(tn_operator* op)
 }
 }  // namespace
 
+namespace {
+template <typename F>
+int dispatch_prec(int precision, F&& f)
+{
+    precision_size(precision);
+    return precision == TN_F64 ? f(double{}) : f(float{});
+}
+void check_comps(int ncomp, const void* p)
+{
+    need(p != nullptr, "NULL argument");
+    need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+}
+}  // namespace
+
+namespace {
+void max_abs_nan(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev, double* mx, int* nan,
+                 void* stream)
+{
+    check_comps(ncomp, a_dev);
+    const auto& L   = shell->impl->level(level);
+    double*     red = shell->impl->red.as<double>();
+    int*        flag = reinterpret_cast<int*>(red + tn::reduction_partials_size() + 4);
+    tn::cuda_check(cudaMemsetAsync(flag, 0, sizeof(int), as_stream(stream)), "clear flag");
+    const int rc = dispatch_prec(precision, [&](auto t) {
+        using T = decltype(t);
+        return tn::max_abs_and_nan<T>(L.nodes(), ncomp, reinterpret_cast<const T* const*>(a_dev), red, flag,
+                                      as_stream(stream));
+    });
+    if (rc) throw tn::Error(tn::kErrCuda, "max-abs launch failed");
+    double h_mx = 0.0;
+    int    h_nan = 0;
+    tn::cuda_check(cudaMemcpyAsync(&h_mx, red, sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)), "readback");
+    tn::cuda_check(cudaMemcpyAsync(&h_nan, flag, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream)), "readback");
+    tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "max-abs sync");
+    if (mx) *mx = h_mx;
+    if (nan) *nan = h_nan != 0;
+}
+}  // namespace
+
+namespace {
+void rotate(tn_shell* shell, int level, int precision, void* const* v_dev, int flag, int mode, void* stream)
+{
+    need(shell, "NULL shell");
+    check_comps(3, v_dev);
+    need(flag >= 0 && flag < 256, "flag must be a ShellBoundaryFlag value");
+    const auto& L  = shell->impl->level(level);
+    const int   rc = dispatch_prec(precision, [&](auto t) {
+        using T = decltype(t);
+        return tn::rotate_normal_tangential<T>(L.nodes(), L.nr(), L.coords<T>(), reinterpret_cast<T* const*>(v_dev),
+                                               flag, mode, as_stream(stream));
+    });
+    if (rc) throw tn::Error(tn::kErrCuda, "rotation launch failed");
+}
+int shell_boundary_flag(int bc_cmb, int bc_surface, int bcf)
+{
+    if (bc_cmb == bcf) return tn::kFlagCMB;
+    if (bc_surface == bcf) return tn::kFlagSurface;
+    return 0;
+}
+}  // namespace
+
+
 extern "C" {
 
 const char* tn_last_error(void) { return g_last_error.c_str(); }
@@ -282,6 +345,7 @@ int tn_epsdivdiv_create(tn_shell* shell, int level, int precision, const void* k
         need(shell && out, "NULL argument");
         auto e = std::make_unique<tn::EpsDivDivOp>();
         init_edd(*e, shell->impl.get(), level, precision, k_nodal_dev, k_cell_dev, bc_cmb, bc_surface, diagonal);
+        e->prepare_penalty(nullptr);
         auto o = new tn_operator;
         o->op  = std::move(e);
         *out   = o;
@@ -364,7 +428,9 @@ int tn_operator_set_boundary_conditions(tn_operator* op, int bc_cmb, int bc_surf
         if (auto* s = dynamic_cast<tn::StokesOp*>(op->op.get())) {
             s->A.bc_cmb = s->B.bc_cmb = s->BT.bc_cmb = bc_cmb;
             s->A.bc_surf = s->B.bc_surf = s->BT.bc_surf = bc_surface;
+            s->A.prepare_penalty(nullptr);
         }
+        if (auto* e = dynamic_cast<tn::EpsDivDivOp*>(op->op.get())) e->prepare_penalty(nullptr);
     });
 }
 
@@ -569,6 +635,138 @@ int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void*
     });
 }
 
+
+/* ---- remaining VectorLike operations ----------------------------------- */
+int tn_vec_invert(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell, "NULL shell");
+        check_comps(ncomp, y_dev);
+        const auto& L  = shell->impl->level(level);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            return tn::invert_inplace<T>(L.nodes(), ncomp, reinterpret_cast<T* const*>(y_dev), as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "invert launch failed");
+    });
+}
+
+int tn_vec_scale(tn_shell* shell, int level, int precision, int ncomp, void* const* y_dev, const void* const* x_dev,
+                 void* stream)
+{
+    return guarded([&] {
+        need(shell && x_dev, "NULL argument");
+        check_comps(ncomp, y_dev);
+        const auto& L  = shell->impl->level(level);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            return tn::scale_inplace<T>(L.nodes(), ncomp, reinterpret_cast<T* const*>(y_dev),
+                                        reinterpret_cast<const T* const*>(x_dev), as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "scale launch failed");
+    });
+}
+
+int tn_vec_max_abs(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev, double* result,
+                   void* stream)
+{
+    return guarded([&] {
+        need(shell && result, "NULL argument");
+        max_abs_nan(shell, level, precision, ncomp, a_dev, result, nullptr, stream);
+    });
+}
+
+int tn_vec_has_nan_or_inf(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev, int* result,
+                          void* stream)
+{
+    return guarded([&] {
+        need(shell && result, "NULL argument");
+        max_abs_nan(shell, level, precision, ncomp, a_dev, nullptr, result, stream);
+    });
+}
+
+int tn_vec_swap(tn_shell* shell, int level, int precision, int ncomp, void* const* a_dev, void* const* b_dev,
+                void* stream)
+{
+    return guarded([&] {
+        need(shell && b_dev, "NULL argument");
+        check_comps(ncomp, a_dev);
+        const auto& L  = shell->impl->level(level);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            return tn::swap_vectors<T>(L.nodes(), ncomp, reinterpret_cast<T* const*>(a_dev),
+                                       reinterpret_cast<T* const*>(b_dev), as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "swap launch failed");
+    });
+}
+
+int tn_vec_cast(int64_t n, int direction, const void* in_dev, void* out_dev, void* stream)
+{
+    return guarded([&] {
+        need(n >= 0 && (n == 0 || (in_dev && out_dev)), "bad arguments");
+        precision_size(direction);
+        if (n == 0) return;
+        const int rc = direction == TN_F64
+                           ? tn::convert_f64_to_f32(n, static_cast<const double*>(in_dev), static_cast<float*>(out_dev),
+                                                    as_stream(stream))
+                           : tn::convert_f32_to_f64(n, static_cast<const float*>(in_dev), static_cast<double*>(out_dev),
+                                                    as_stream(stream));
+        if (rc) throw tn::Error(tn::kErrCuda, "cast launch failed");
+    });
+}
+
+/* ---- boundary treatment of right-hand sides ----------------------------- */
+int tn_vec_assign_masked(tn_shell* shell, int level, int precision, int ncomp, void* const* v_dev, int flag,
+                         double value, void* stream)
+{
+    return guarded([&] {
+        need(shell, "NULL shell");
+        check_comps(ncomp, v_dev);
+        need(flag >= 0 && flag < 256, "flag must be a ShellBoundaryFlag value");
+        const auto& L  = shell->impl->level(level);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            return tn::assign_masked<T>(L.nodes(), L.nr(), ncomp, reinterpret_cast<T* const*>(v_dev), flag,
+                                        static_cast<T>(value), as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "assign launch failed");
+    });
+}
+
+int tn_vec_rotate_normal_tangential(tn_shell* shell, int level, int precision, void* const* v_dev, int flag,
+                                    int direction, void* stream)
+{
+    return guarded([&] {
+        need(direction == 0 || direction == 1, "direction must be 0 or 1");
+        rotate(shell, level, precision, v_dev, flag, direction, stream);
+    });
+}
+
+int tn_vec_freeslip_project(tn_shell* shell, int level, int precision, void* const* v_dev, int flag, void* stream)
+{
+    return guarded([&] { rotate(shell, level, precision, v_dev, flag, 2, stream); });
+}
+
+int tn_stokes_rhs_enforce(tn_shell* shell, int level, int precision, int bc_cmb, int bc_surface, void* const* u_dev,
+                          void* stream)
+{
+    return guarded([&] {
+        need(shell, "NULL shell");
+        check_bcs(bc_cmb, bc_surface);
+        check_comps(3, u_dev);
+        const auto& L     = shell->impl->level(level);
+        const int   fdir  = shell_boundary_flag(bc_cmb, bc_surface, TN_DIRICHLET);
+        const int   ffs   = shell_boundary_flag(bc_cmb, bc_surface, TN_FREESLIP);
+        const int   rc    = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            auto* v = reinterpret_cast<T* const*>(u_dev);
+            if (tn::assign_masked<T>(L.nodes(), L.nr(), 3, v, fdir, T(0), as_stream(stream)) != 0) return -1;
+            return tn::rotate_normal_tangential<T>(L.nodes(), L.nr(), L.coords<T>(), v, ffs, 2, as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "right-hand-side launch failed");
+    });
+}
 
 /* ---- stored matrices and Galerkin coarse operators ---------------------- */
 int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream)

@@ -1,10 +1,12 @@
 // Host runtime: device mesh construction and operator dispatch.
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
 
 #include <type_traits>
 
+#include "tn_boundary.hpp"
 #include "tn_runtime.hpp"
 
 namespace tn {
@@ -164,6 +166,77 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st)
     coarse.baked32_valid = false;
 }
 
+void EpsDivDivOp::prepare_penalty(cudaStream_t st)
+{
+    if (!penalty_active() || pen_modes.get() != nullptr) return;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cuda_check(cudaStreamIsCapturing(st, &cap), "capture status");
+    if (cap != cudaStreamCaptureStatusNone)
+        throw Error(kErrState, "the free-slip null-space modes must be built before stream capture");
+    const DeviceLevel& L  = lvl();
+    const int64_t      n  = L.nodes();
+    const uint8_t*     ow = L.owned_lat.as<uint8_t>();
+    double*            red = shell->red.as<double>();
+    DevBuf             m64(sizeof(double) * 9 * static_cast<size_t>(n));
+    if (null_space_modes_raw(n, L.nr(), L.coords<double>(), L.radii<double>(), m64.as<double>(), st) != 0)
+        throw Error(kErrCuda, "null-space mode launch failed");
+    auto mode = [&](int a, double** out) {
+        for (int d = 0; d < 3; ++d) out[d] = m64.as<double>() + (static_cast<int64_t>(a) * 3 + d) * n;
+    };
+    auto dot = [&](int a, int b) {
+        double* ma[3];
+        double* mb[3];
+        mode(a, ma);
+        mode(b, mb);
+        const double* ca[3] = {ma[0], ma[1], ma[2]};
+        const double* cb[3] = {mb[0], mb[1], mb[2]};
+        if (masked_dot<double>(n, L.nr(), 3, ow, ca, cb, red, red + 8, st) != 0)
+            throw Error(kErrCuda, "dot launch failed");
+        double h = 0.0;
+        cuda_check(cudaMemcpyAsync(&h, red, sizeof(double), cudaMemcpyDeviceToHost, st), "dot readback");
+        cuda_check(cudaStreamSynchronize(st), "dot sync");
+        return h;
+    };
+    // modified Gram-Schmidt with owned-node dots, then normalisation (epsilon_divdiv_kerngen.hpp:403-440)
+    for (int i = 0; i < 3; ++i) {
+        double* mi[3];
+        mode(i, mi);
+        const double* ci[3] = {mi[0], mi[1], mi[2]};
+        for (int j = 0; j < i; ++j) {
+            double* mj[3];
+            mode(j, mj);
+            const double* cj[3] = {mj[0], mj[1], mj[2]};
+            const double  c[2]  = {1.0, -dot(i, j)};
+            if (lincomb<double>(n, 3, mi, 0.0, 2, c, ci, cj, nullptr, st) != 0)
+                throw Error(kErrCuda, "lincomb launch failed");
+        }
+        const double inv = 1.0 / std::sqrt(dot(i, i));
+        if (lincomb<double>(n, 3, mi, 0.0, 1, &inv, ci, nullptr, nullptr, st) != 0)
+            throw Error(kErrCuda, "lincomb launch failed");
+    }
+    if (precision == 0) {
+        pen_modes = std::move(m64);
+    } else {
+        pen_modes.alloc(sizeof(float) * 9 * static_cast<size_t>(n));
+        if (convert_f64_to_f32(9 * n, m64.as<double>(), pen_modes.as<float>(), st) != 0)
+            throw Error(kErrCuda, "conversion launch failed");
+        cuda_check(cudaStreamSynchronize(st), "mode conversion");
+    }
+    pen_scratch.alloc(sizeof(double) * (penalty_partials_size() + 4));
+}
+
+template <typename T>
+void EpsDivDivOp::add_penalty(const T* const* src, T* const* dst, cudaStream_t st)
+{
+    if (!penalty_active() || diagonal) return;
+    prepare_penalty(st);
+    const DeviceLevel& L = lvl();
+    double*            ps = pen_scratch.as<double>();
+    if (penalty_apply<T>(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), src, dst, pen_modes.as<T>(), kPenaltyEpsilon,
+                         ps + 4, ps, st) != 0)
+        throw Error(kErrCuda, "penalty launch failed");
+}
+
 template <typename T>
 void EpsDivDivOp::vjp_logeta(const T* const* u, const T* const* lam, T* grad_cell, cudaStream_t st) const
 {
@@ -212,6 +285,7 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
                                                        : static_cast<const T*>(baked64.get());
             if (gca_apply_add<T>(L.nl(), L.nr(), m, src, dst, st) != 0)
                 throw Error(kErrCuda, "stored apply launch failed");
+            add_penalty<T>(src, dst, st);
         }
         if (comm_mode == 1) iface<T>(L, 3, dst, st);
         return;
@@ -238,6 +312,7 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
     p.err      = shell->err_word();
     const int rc = epsdivdiv_apply<T>(p, st);
     if (rc != 0) throw Error(kErrCuda, "epsdivdiv launch failed (" + std::to_string(rc) + ")");
+    add_penalty<T>(src, dst, st);
     if (comm_mode == 1) iface<T>(L, 3, dst, st);
 }
 template void EpsDivDivOp::apply_t<double>(const double* const*, double* const*, cudaStream_t);

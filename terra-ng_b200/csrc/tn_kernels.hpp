@@ -135,6 +135,8 @@ int masked_dot(int64_t n, int nr, int ncomp, const uint8_t* owned_lat, const T* 
 // out = max |a| ; out_flags = 1 if any NaN/Inf
 template <typename T>
 int max_abs_and_nan(int64_t n, int ncomp, const T* const* a, double* out_dev, int* nan_dev, cudaStream_t stream);
+// doubles of the shell's reduction scratch used by masked_dot / max_abs_and_nan partials
+int reduction_partials_size();
 // precision conversion
 int convert_f64_to_f32(int64_t n, const double* in, float* out, cudaStream_t stream);
 int convert_f32_to_f64(int64_t n, const float* in, double* out, cudaStream_t stream);

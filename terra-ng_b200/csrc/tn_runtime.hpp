@@ -214,6 +214,10 @@ struct EpsDivDivOp : Operator {
     bool   diagonal = false;
     int    tile_y = 0, chunk_x = 0;
 
+    // free slip on both boundaries: orthonormal rotation modes (3 modes x 3 components x nodes, in
+    // `precision`) and the scratch of the penalty dst += eps sum_i (n_i^T src) n_i
+    DevBuf pen_modes, pen_scratch;
+
     bool   stored = false;
     DevBuf mats;              // FP64 unbaked element matrices [342][cells]
     DevBuf baked64, baked32;  // boundary-baked copies (built lazily)
@@ -228,6 +232,11 @@ struct EpsDivDivOp : Operator {
     // backward of the apply: grad_cell = d(lambda^T A u)/d log(eta_cell) (Q0 only)
     template <typename T>
     void vjp_logeta(const T* const* u, const T* const* lam, T* grad_cell, cudaStream_t st) const;
+    // free-slip/free-slip null-space penalty (epsilon_divdiv_kerngen.hpp:324-445, :711-785)
+    bool penalty_active() const { return bc_cmb == 2 && bc_surf == 2; }
+    void prepare_penalty(cudaStream_t st);  // builds the modes (synchronous); no-op unless active or built
+    template <typename T>
+    void add_penalty(const T* const* src, T* const* dst, cudaStream_t st);
     // stored-matrix helpers
     void ensure_baked(bool need32, cudaStream_t st);
     void set_stored_matrices_from_coefficient(cudaStream_t st);  // element matrices of this level

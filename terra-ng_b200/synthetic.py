@@ -111,19 +111,15 @@ def buoyancy_rhs(shell: "T.Shell", level: int, temp, bc_cmb: int, bc_surface: in
 
 
 def enforce_boundary(shell: "T.Shell", level: int, f, bc_cmb: int, bc_surface: int):
-    """Zero Dirichlet rows and remove free-slip normal components
-    (strong_algebraic_dirichlet_enforcement.hpp:114-123,
+    """Zero the Dirichlet boundary rows and remove the free-slip normal components of every boundary carrying
+    that condition (the library's assign-masked and free-slip projection kernels, tn_vec_assign_masked /
+    tn_vec_freeslip_project: strong_algebraic_dirichlet_enforcement.hpp:114-123,
     strong_algebraic_freeslip_enforcement.hpp:22-38)."""
-    import torch
-
-    coords, _ = _geometry(shell, level)
-    n = torch.tensor(coords, device="cuda").permute(3, 0, 1, 2)
-    for side, bc in ((0, bc_cmb), (-1, bc_surface)):
+    for flag, bc in ((T.FLAG_CMB, bc_cmb), (T.FLAG_SURFACE, bc_surface)):
         if bc == T.DIRICHLET:
-            f[..., side] = 0.0
+            T.vec_assign_masked(shell, level, f, flag, 0.0)
         elif bc == T.FREESLIP:
-            dn = (f[..., side] * n).sum(0)
-            f[..., side] -= dn[None] * n
+            T.vec_freeslip_project(shell, level, f, flag)
     return f
 
 

@@ -129,6 +129,16 @@ def load(path: str = LIB_PATH):
         "tn_solver_inverse_diagonal": ([vp, i, vpp, vp], i),
         "tn_solver_coarse_stats": ([vp, dp], i),
         "tn_solver_level_matrices": ([vp, i, vp], i),
+        "tn_vec_invert": ([vp, i, i, i, vpp, vp], i),
+        "tn_vec_scale": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_vec_max_abs": ([vp, i, i, i, vpp, dp, vp], i),
+        "tn_vec_has_nan_or_inf": ([vp, i, i, i, vpp, ctypes.POINTER(i), vp], i),
+        "tn_vec_swap": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_vec_cast": ([ctypes.c_int64, i, vp, vp, vp], i),
+        "tn_vec_assign_masked": ([vp, i, i, i, vpp, i, d, vp], i),
+        "tn_vec_rotate_normal_tangential": ([vp, i, i, vpp, i, i, vp], i),
+        "tn_vec_freeslip_project": ([vp, i, i, vpp, i, vp], i),
+        "tn_stokes_rhs_enforce": ([vp, i, i, i, i, vpp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -469,6 +479,81 @@ def restrict(shell: Shell, fine_level: int, fine, coarse, stream=None):
     _check(load().tn_restrict(shell.handle, fine_level % shell.num_levels, _prec(cf[0].dtype), len(cf), _ptrs(cf),
                               _ptrs(cc), _stream(stream)))
     return coarse
+
+
+FLAG_INNER, FLAG_BOUNDARY, FLAG_CMB, FLAG_SURFACE = 1, 2, 6, 10
+
+
+def vec_invert(shell: Shell, level: int, y, stream=None):
+    cy = _comps(y)
+    _check(load().tn_vec_invert(shell.handle, level % shell.num_levels, _prec(cy[0].dtype), len(cy), _ptrs(cy),
+                                _stream(stream)))
+    return y
+
+
+def vec_scale(shell: Shell, level: int, y, x, stream=None):
+    cy, cx = _comps(y), _comps(x)
+    _check(load().tn_vec_scale(shell.handle, level % shell.num_levels, _prec(cy[0].dtype), len(cy), _ptrs(cy),
+                               _ptrs(cx), _stream(stream)))
+    return y
+
+
+def vec_max_abs(shell: Shell, level: int, a, stream=None) -> float:
+    ca = _comps(a)
+    out = ctypes.c_double()
+    _check(load().tn_vec_max_abs(shell.handle, level % shell.num_levels, _prec(ca[0].dtype), len(ca), _ptrs(ca),
+                                 ctypes.byref(out), _stream(stream)))
+    return out.value
+
+
+def vec_has_nan_or_inf(shell: Shell, level: int, a, stream=None) -> bool:
+    ca = _comps(a)
+    out = ctypes.c_int()
+    _check(load().tn_vec_has_nan_or_inf(shell.handle, level % shell.num_levels, _prec(ca[0].dtype), len(ca),
+                                        _ptrs(ca), ctypes.byref(out), _stream(stream)))
+    return bool(out.value)
+
+
+def vec_swap(shell: Shell, level: int, a, b, stream=None):
+    ca, cb = _comps(a), _comps(b)
+    _check(load().tn_vec_swap(shell.handle, level % shell.num_levels, _prec(ca[0].dtype), len(ca), _ptrs(ca),
+                              _ptrs(cb), _stream(stream)))
+
+
+def vec_cast(src, out, stream=None):
+    """FP64 -> FP32 or FP32 -> FP64 copy of a contiguous tensor (tn_vec_cast)."""
+    _check(load().tn_vec_cast(src.numel(), _prec(src.dtype), ctypes.c_void_p(src.data_ptr()),
+                              ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+    return out
+
+
+def vec_assign_masked(shell: Shell, level: int, v, flag: int, value: float = 0.0, stream=None):
+    cv = _comps(v)
+    _check(load().tn_vec_assign_masked(shell.handle, level % shell.num_levels, _prec(cv[0].dtype), len(cv),
+                                       _ptrs(cv), flag, value, _stream(stream)))
+    return v
+
+
+def vec_rotate_normal_tangential(shell: Shell, level: int, v, flag: int, direction: int, stream=None):
+    cv = _comps(v)
+    _check(load().tn_vec_rotate_normal_tangential(shell.handle, level % shell.num_levels, _prec(cv[0].dtype),
+                                                  _ptrs(cv), flag, direction, _stream(stream)))
+    return v
+
+
+def vec_freeslip_project(shell: Shell, level: int, v, flag: int, stream=None):
+    cv = _comps(v)
+    _check(load().tn_vec_freeslip_project(shell.handle, level % shell.num_levels, _prec(cv[0].dtype), _ptrs(cv),
+                                          flag, _stream(stream)))
+    return v
+
+
+def stokes_rhs_enforce(shell: Shell, level: int, u, bc_cmb: int, bc_surface: int, stream=None):
+    """The application's right-hand-side boundary treatment on the 3 velocity components (tn_stokes_rhs_enforce)."""
+    cu = _comps(u)
+    _check(load().tn_stokes_rhs_enforce(shell.handle, level % shell.num_levels, _prec(cu[0].dtype), bc_cmb,
+                                        bc_surface, _ptrs(cu), _stream(stream)))
+    return u
 
 
 def solver_options(**kw) -> SolverOptions:

@@ -16,9 +16,11 @@ def pytest_configure(config):
 def _ensure_built():
     import build as product_build  # terra-ng_b200/build.py
     import oracle
+    import ref
 
     product_build.build()
     oracle.build()
+    ref.build()  # the reference compiled as a checker (only where its source tree is present)
 
 
 _ensure_built()

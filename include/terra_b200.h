@@ -309,9 +309,16 @@ typedef struct tn_solver_options {
                                            Jacobi::solve_impl, jacobi.hpp:51-60, chebyshev_iterations steps)
                                            (TN_SMOOTHER_CHEBYSHEV) */
     double   jacobi_omega;              /* damped-Jacobi relaxation omega (1.0, the reference's default) */
+    int      coarse_solver;             /* coarsest-level solve: TN_COARSE_PCG (the reference's PCG with
+                                           coarse_max_iterations / coarse_relative_tolerance, pcg.hpp:81-169) or
+                                           TN_COARSE_DENSE (the assembled coarsest operator inverted once at
+                                           set-up, an exact solve by one dense product per V-cycle; coarsest
+                                           levels up to 16384 unknowns) (TN_COARSE_PCG) */
 } tn_solver_options;
 #define TN_SMOOTHER_CHEBYSHEV 0
 #define TN_SMOOTHER_JACOBI 1
+#define TN_COARSE_PCG 0
+#define TN_COARSE_DENSE 1
 void tn_solver_options_default(tn_solver_options* opts);
 /* Stokes solve on velocity_level / velocity_level-1 (StokesContext,
  * apps/mantlecirculation/src/stokes_solver.hpp:325-609): FGMRES(m) with the
@@ -330,6 +337,18 @@ int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* e
 int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
                               int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
                               tn_solver** out);
+/* The velocity multigrid as a solver (Multigrid, src/terra/linalg/solvers/
+ * multigrid.hpp:42-280, with the hierarchy the application builds, apps/
+ * mantlecirculation/src/stokes_solver.hpp:351-557): levels 0..level of the
+ * shell, smoother = Chebyshev(chebyshev_order, chebyshev_iterations,
+ * power_iterations) or damped Jacobi (smoother, jacobi_omega), coarse =
+ * coarse_solver, Galerkin or rediscretised coarse operators (gca). A solve runs
+ * up to max_iterations times num_vcycles V-cycles from the initial guess in x,
+ * recording the relative residual after each (the reference's statistics rows)
+ * and stopping at relative_tolerance / absolute_tolerance. 3 components. */
+int tn_multigrid_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+                               int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
+                               tn_solver** out);
 void tn_solver_destroy(tn_solver* solver);
 /* solve_impl(A, x, b): x_dev holds the initial guess and receives the
  * solution; 4 components (u_x, u_y, u_z, p) for a Stokes solver, 3 for a

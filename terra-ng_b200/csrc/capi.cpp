@@ -113,6 +113,8 @@ tn::MgOptions mg_options(const tn_solver_options& o)
     m.seed            = o.seed;
     m.smoother        = o.smoother;
     m.jacobi_omega    = o.jacobi_omega;
+    m.coarse_dense    = o.coarse_solver == TN_COARSE_DENSE ? 1 : 0;
+    need(o.coarse_solver == TN_COARSE_PCG || o.coarse_solver == TN_COARSE_DENSE, "unknown coarse solver");
     need(o.gca == 0 || o.gca == 1, "gca must be 0 or 1");
     need(o.smoother == TN_SMOOTHER_CHEBYSHEV || o.smoother == TN_SMOOTHER_JACOBI, "unknown smoother");
     need(o.jacobi_omega > 0.0, "jacobi_omega must be positive");
@@ -844,6 +846,7 @@ void tn_solver_options_default(tn_solver_options* o)
     o->cuda_graphs               = 1;
     o->smoother                  = TN_SMOOTHER_CHEBYSHEV;
     o->jacobi_omega              = 1.0;
+    o->coarse_solver             = TN_COARSE_PCG;
 }
 
 int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,
@@ -874,9 +877,10 @@ int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* e
     });
 }
 
-int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+namespace {
+int velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
                               int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
-                              tn_solver** out)
+                           tn_solver** out, bool multigrid_only)
 {
     return guarded([&] {
         need(shell && out, "NULL argument");
@@ -889,12 +893,31 @@ int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_noda
         vo.rtol     = o.relative_tolerance;
         vo.atol     = o.absolute_tolerance;
         vo.mg       = mg_options(o);
+        vo.multigrid_only = multigrid_only;
         auto s      = std::make_unique<tn_solver>();
         s->shell    = shell;
         s->velocity = std::make_unique<tn::VelocitySolver>(shell->impl.get(), level, eta_nodal_dev, eta_cell_dev,
                                                            bc_cmb, bc_surface, vo, as_stream(stream));
         *out = s.release();
     });
+}
+
+}  // namespace
+
+int tn_velocity_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+                              int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
+                              tn_solver** out)
+{
+    return velocity_solver_create(shell, level, eta_nodal_dev, eta_cell_dev, bc_cmb, bc_surface, opts, stream, out,
+                                  false);
+}
+
+int tn_multigrid_solver_create(tn_shell* shell, int level, const double* eta_nodal_dev, const double* eta_cell_dev,
+                               int bc_cmb, int bc_surface, const tn_solver_options* opts, void* stream,
+                               tn_solver** out)
+{
+    return velocity_solver_create(shell, level, eta_nodal_dev, eta_cell_dev, bc_cmb, bc_surface, opts, stream, out,
+                                  true);
 }
 
 void tn_solver_destroy(tn_solver* s) { delete s; }

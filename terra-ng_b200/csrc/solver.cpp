@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <string>
 #include <type_traits>
 
 #include "tn_solver.hpp"
@@ -203,6 +204,8 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
         }
     }
 
+    if (o.coarse_dense) build_dense_coarse(st);
+
     // FP32 operators where the apply is matrix-free
     if (o.fp32) {
         for (int l = 1; l <= fine_; ++l) {
@@ -280,6 +283,67 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     cpart_.alloc(sizeof(double) * coarse_pcg_partials_size());
     cstats_.alloc(sizeof(double) * 4);
     cuda_check(cudaMemset(cstats_.get(), 0, sizeof(double) * 4), "zero stats");
+}
+
+// Dense inverse of the coarsest operator (coarse_dense.cu): unique-node numbering from the ownership flags and
+// the duplicate classes, one column per unknown from the stored operator applied to a unit vector that is 1 on
+// every copy of the unknown, then in-place Gauss-Jordan inversion. Synchronous set-up.
+void VelocityMultigrid::build_dense_coarse(cudaStream_t st)
+{
+    const DeviceLevel& L0 = sh_->level(0);
+    const ShellLevel&  h  = L0.host;
+    const int          nr = L0.nr();
+    const int64_t      nodes = L0.nodes();
+    const int          nlat  = static_cast<int>(h.owned_lat.size());
+    std::vector<int32_t> owner(nlat);
+    for (int c = 0; c < nlat; ++c) owner[c] = c;
+    for (size_t k = 0; k + 1 < h.dup_offset.size(); ++k) {
+        int32_t own = -1;
+        for (int32_t m = h.dup_offset[k]; m < h.dup_offset[k + 1]; ++m)
+            if (h.owned_lat[h.dup_members[m]]) own = h.dup_members[m];
+        if (own < 0) throw Error(kErrState, "a duplicate class without an owned copy");
+        for (int32_t m = h.dup_offset[k]; m < h.dup_offset[k + 1]; ++m) owner[h.dup_members[m]] = own;
+    }
+    std::vector<int32_t> uid_owned(static_cast<size_t>(nodes), -1), rep, uid(static_cast<size_t>(nodes));
+    for (int c = 0; c < nlat; ++c)
+        if (h.owned_lat[c])
+            for (int r = 0; r < nr; ++r) {
+                uid_owned[static_cast<size_t>(c) * nr + r] = static_cast<int32_t>(rep.size());
+                rep.push_back(static_cast<int32_t>(c * nr + r));
+            }
+    for (int c = 0; c < nlat; ++c)
+        for (int r = 0; r < nr; ++r) uid[static_cast<size_t>(c) * nr + r] = uid_owned[static_cast<size_t>(owner[c]) * nr + r];
+    knu_         = static_cast<int>(rep.size());
+    const int nd = 3 * knu_;
+    if (nd > kDenseCoarseMaxUnknowns)
+        throw Error(kErrUnsupported, "the coarsest level is too large for the dense coarse solve (" +
+                                         std::to_string(nd) + " unknowns)");
+    chk(dense_coarse_prepare(nd), "dense coarse configuration");
+    kuid_ = upload(uid);
+    krep_ = upload(rep);
+    ky_.alloc(sizeof(double) * nd);
+    kinv_.alloc(sizeof(double) * static_cast<size_t>(nd) * nd);
+    DevBuf        colk(sizeof(double) * nd);
+    const VecDesc v0 = velocity_desc(L0);
+    DVec<double>  e, y;
+    e.alloc(v0);
+    y.alloc(v0);
+    const int64_t s      = v0.seg[0].stride;
+    EpsDivDivOp&  A0     = *ops64_[0];
+    const int     amode  = A0.apply_mode, cmode = A0.comm_mode;
+    A0.apply_mode        = 0;
+    A0.comm_mode         = 1;
+    const double* src[3] = {e.data(), e.data() + s, e.data() + 2 * s};
+    double*       dst[3] = {y.data(), y.data() + s, y.data() + 2 * s};
+    for (int j = 0; j < nd; ++j) {
+        chk(dense_unit_vector(nodes, s, knu_, kuid_.as<int32_t>(), j, e.data(), st), "unit vector");
+        A0.apply_t<double>(src, dst, st);
+        chk(dense_gather_column(knu_, s, krep_.as<int32_t>(), y.data(), j, kinv_.as<double>(), st), "column");
+    }
+    A0.apply_mode = amode;
+    A0.comm_mode  = cmode;
+    chk(dense_invert_spd(nd, kinv_.as<double>(), colk.as<double>(), st), "inversion");
+    cuda_check(cudaStreamSynchronize(st), "dense coarse set-up");
 }
 
 double VelocityMultigrid::power_iteration(int l, int iterations, uint64_t seed, cudaStream_t st)
@@ -420,6 +484,14 @@ void VelocityMultigrid::coarse_solve(T* x, const T* b, cudaStream_t st)
         chk(convert_f32_to_f64(nt, reinterpret_cast<const float*>(b), cb_.data(), st), "widen");
         xd = cx_.data();
         bd = cb_.data();
+    }
+    if (kinv_.get() != nullptr) {
+        chk(dense_coarse_solve(L0.nodes(), pad64(L0.nodes()), knu_, kuid_.as<int32_t>(), krep_.as<int32_t>(),
+                               kinv_.as<double>(), bd, ky_.as<double>(), xd, st),
+            "dense coarse solve");
+        if (!std::is_same<T, double>::value)
+            chk(convert_f64_to_f32(nt, cx_.data(), reinterpret_cast<float*>(x), st), "narrow");
+        return;
     }
     EpsDivDivOp& A0 = *ops64_[0];
     A0.ensure_baked(false, st);
@@ -1033,6 +1105,31 @@ bool VelocitySolver::solve(double* const* u, const double* const* f, cudaStream_
     apply(x_, r_);
     const double one_m[2] = {1.0, -1.0};
     lin<double>(nt, r_.data(), 0.0, 2, one_m, b_.data(), r_.data(), st);
+    if (opt_.multigrid_only) {
+        // Multigrid::solve_impl with statistics (multigrid.hpp:233-279): residual before and after each cycle
+        chk(vec_dot<double>(vd_, r_.data(), r_.data(), scratch_.s(0), scratch_.rs(), true, st), "norm");
+        scratch_.fetch(1, st);
+        const double init = scratch_.host[0];
+        history.push_back(1.0);
+        converged = init < opt_.atol;
+        for (int it = 1; it <= opt_.max_iter && !converged; ++it) {
+            mg_->solve64(x_.data(), b_.data(), st);
+            apply(x_, r_);
+            lin<double>(nt, r_.data(), 0.0, 2, one_m, b_.data(), r_.data(), st);
+            chk(vec_dot<double>(vd_, r_.data(), r_.data(), scratch_.s(0), scratch_.rs(), true, st), "norm");
+            scratch_.fetch(1, st);
+            const double res = scratch_.host[0];
+            iterations       = it;
+            final_relres     = init > 0.0 ? res / init : 0.0;
+            history.push_back(final_relres);
+            if (!std::isfinite(res)) break;
+            converged = final_relres <= opt_.rtol || res < opt_.atol;
+        }
+        for (int c = 0; c < 3; ++c)
+            cuda_check(cudaMemcpyAsync(u[c], x_.comp(0, c), bytes, cudaMemcpyDeviceToDevice, st), "copy out");
+        cuda_check(cudaStreamSynchronize(st), "synchronize");
+        return converged;
+    }
     precondition(st);
     cuda_check(cudaMemcpyAsync(p_.data(), z_.data(), sizeof(double) * nt, cudaMemcpyDeviceToDevice, st), "copy");
     chk(vec_dot<double>(vd_, r_.data(), r_.data(), scratch_.s(0), scratch_.rs(), true, st), "norm");

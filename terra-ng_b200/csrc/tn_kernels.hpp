@@ -291,6 +291,20 @@ int coarse_pcg_uses_full_matrices(int nl, int nr, int num_classes, int num_membe
 // full[(w * 18 + a) * 18 + b][cell] = packed[w * 171 + pidx(a, b)][cell], nc cells
 int coarse_matrices_unpack(int nc, const double* packed, double* full, cudaStream_t st);
 int coarse_pcg_partials_size();
+
+// Dense direct coarsest solve (coarse_dense.cu). Unknown (c, u) = c * nu + u; uid maps every stored node to
+// its unique node, rep each unique node to its owned copy; vectors are 3 FP64 components `stride` apart.
+constexpr int kDenseCoarseMaxUnknowns = 16384;  // 2 GB of FP64 inverse; the GEMV stages the rhs in shared memory
+int dense_unit_vector(int64_t nodes, int64_t stride, int nu, const int32_t* uid, int dof, double* v, cudaStream_t st);
+int dense_gather_column(int nu, int64_t stride, const int32_t* rep, const double* y, int col, double* K,
+                        cudaStream_t st);
+// in-place inverse of an SPD n x n matrix (Gauss-Jordan, no pivoting); colk: n doubles of scratch
+int dense_invert_spd(int64_t n, double* A, double* colk, cudaStream_t st);
+// kernel attributes for `unknowns` (call outside stream capture)
+int dense_coarse_prepare(int unknowns);
+// x = Kinv b (gathered at rep, scattered to every copy); y: 3 * nu doubles of scratch
+int dense_coarse_solve(int64_t nodes, int64_t stride, int nu, const int32_t* uid, const int32_t* rep,
+                       const double* Kinv, const double* b, double* y, double* x, cudaStream_t st);
 int coarse_pcg_cluster_size();
 
 }  // namespace tn

@@ -53,6 +53,7 @@ struct MgOptions {
     uint64_t seed = 12345;  // power-iteration start vectors
     int      smoother     = 0;    // 0: Chebyshev (cheb_order, cheb_iters), 1: damped Jacobi (cheb_iters steps)
     double   jacobi_omega = 1.0;  // Jacobi relaxation
+    int      coarse_dense = 0;    // 0: coarsest CG (the reference's PCG); 1: dense inverse built once, exact solve
 };
 
 // Velocity multigrid (Multigrid, multigrid.hpp:216-432) over levels 0..fine of
@@ -93,6 +94,7 @@ class VelocityMultigrid {
     void vcycle(int l, T* x, const T* b, cudaStream_t st);
     template <typename T>
     void coarse_solve(T* x, const T* b, cudaStream_t st);
+    void build_dense_coarse(cudaStream_t st);  // kinv_ = inverse of the assembled coarsest operator
 
     const Shell*                              sh_;
     int                                       fine_;
@@ -106,6 +108,8 @@ class VelocityMultigrid {
     DVec<double>                              cx_, cb_, cr_, cp_, cap_;  // coarsest CG vectors
     DevBuf                                    cpart_, cstats_;
     DevBuf                                    cfull_;  // row-major coarsest matrices (replicated CG)
+    DevBuf                                    kinv_, kuid_, krep_, ky_;  // dense coarsest solve
+    int                                       knu_ = 0;                  // unique coarsest nodes
     DVec<double>                              ext64_[2];
     DVec<float>                               ext32_[2];
 };
@@ -189,11 +193,15 @@ class StokesSolver {
 struct VelocitySolverOptions {
     int       max_iter = 100;
     double    rtol = 1e-8, atol = 1e-16;
+    bool      multigrid_only = false;  // Multigrid::solve_impl: repeated V-cycles (num_vcycles each) instead of CG
     MgOptions mg;
 };
 
 // PCG (pcg.hpp:81-169) on the epsilon-div-div operator with the velocity
-// multigrid as preconditioner, each application starting from z = 0.
+// multigrid as preconditioner, each application starting from z = 0; or, with
+// multigrid_only, the multigrid as the solver (Multigrid::solve_impl,
+// multigrid.hpp:216-280): V-cycles from the caller's initial guess with the
+// residual recorded after each, stopping at the relative tolerance.
 class VelocitySolver {
   public:
     VelocitySolver(const Shell* sh, int level, const double* eta_nodal, const double* eta_cell, int bc_cmb,

@@ -28,6 +28,7 @@ STORED_OFF, STORED_FULL = 0, 1
 
 
 SMOOTHER_CHEBYSHEV, SMOOTHER_JACOBI = 0, 1
+COARSE_PCG, COARSE_DENSE = 0, 1
 
 
 class SolverOptions(ctypes.Structure):
@@ -53,6 +54,7 @@ class SolverOptions(ctypes.Structure):
         ("cuda_graphs", ctypes.c_int),
         ("smoother", ctypes.c_int),
         ("jacobi_omega", ctypes.c_double),
+        ("coarse_solver", ctypes.c_int),
     ]
 
 
@@ -115,6 +117,8 @@ def load(path: str = LIB_PATH):
                                      ctypes.POINTER(vp)], i),
         "tn_velocity_solver_create": ([vp, i, vp, vp, i, i, ctypes.POINTER(SolverOptions), vp, ctypes.POINTER(vp)],
                                       i),
+        "tn_multigrid_solver_create": ([vp, i, vp, vp, i, i, ctypes.POINTER(SolverOptions), vp, ctypes.POINTER(vp)],
+                                       i),
         "tn_solver_destroy": ([vp], None),
         "tn_solver_solve": ([vp, vpp, vpp, vp], i),
         "tn_solver_result": ([vp, ctypes.POINTER(i), dp, ctypes.POINTER(i)], i),
@@ -677,4 +681,18 @@ class VelocitySolver(_Solver):
         _check(load().tn_velocity_solver_create(shell.handle, self.level, _opt_ptr(eta), _opt_ptr(eta_cell), bc_cmb,
                                                 bc_surface, ctypes.byref(self.options), _stream(stream),
                                                 ctypes.byref(h)))
+        self._h = h
+
+
+class MultigridSolver(VelocitySolver):
+    """The velocity multigrid used as the solver (tn_multigrid_solver_create): repeated V-cycles."""
+
+    def __init__(self, shell: Shell, level: int = -1, eta=None, eta_cell=None, bc_cmb=DIRICHLET,
+                 bc_surface=DIRICHLET, stream=None, **options):
+        self.shell, self.level = shell, level % shell.num_levels
+        self.options = solver_options(**options)
+        h = ctypes.c_void_p()
+        _check(load().tn_multigrid_solver_create(shell.handle, self.level, _opt_ptr(eta), _opt_ptr(eta_cell), bc_cmb,
+                                                 bc_surface, ctypes.byref(self.options), _stream(stream),
+                                                 ctypes.byref(h)))
         self._h = h

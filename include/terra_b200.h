@@ -180,6 +180,19 @@ int tn_prolongate_add(tn_shell* shell, int fine_level, int precision, int ncomp,
                       void* const* fine_dev, void* stream);
 int tn_restrict(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
                 void* const* coarse_dev, void* stream);
+/* Linear transfers that interpolate affine functions exactly on the curved
+ * shell (ProlongationLinear / RestrictionLinear, src/terra/fe/wedge/operators/
+ * shell/prolongation_linear.hpp, restriction_linear.hpp, weights of
+ * prolongation_linear_weights, src/terra/fe/wedge/shell/grid_transfer_linear.hpp:
+ * 13-157), applied per component: fine += P coarse, and coarse = P^T (owned
+ * fine) with the coarse interface sum. The weights of the fine level are
+ * computed on first use (synchronous; before any stream capture). */
+#define TN_TRANSFER_CONSTANT 0
+#define TN_TRANSFER_LINEAR 1
+int tn_prolongate_linear_add(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* coarse_dev,
+                             void* const* fine_dev, void* stream);
+int tn_restrict_linear(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
+                       void* const* coarse_dev, void* stream);
 
 /* ---- nodal-vector kernels (VectorQ1Vec / VectorQ1Scalar, src/terra/linalg/
  * vector_q1.hpp:20-304; kernels/common/grid_operations.hpp) --------------- */
@@ -274,6 +287,11 @@ int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream);
  * (FP64 coefficient). The coarse operator applies in its own precision.
  * Synchronous. */
 int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream);
+/* TwoGridGCA with its interpolation_mode argument (gca.hpp:72-78):
+ * TN_TRANSFER_CONSTANT (InterpolationMode::Constant, tn_gca_build) or
+ * TN_TRANSFER_LINEAR (InterpolationMode::Linear: P from the linear-transfer
+ * weights, gca.hpp:231-243, :327-342). Synchronous. */
+int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, void* stream);
 /* get_local_matrix for every cell: host array (10, nl-1, nl-1, nr-1, 2, 18, 18),
  * dimension-wise ordering (row = node + 6 * component), without boundary
  * treatment. Synchronous. */
@@ -314,6 +332,10 @@ typedef struct tn_solver_options {
                                            TN_COARSE_DENSE (the assembled coarsest operator inverted once at
                                            set-up, an exact solve by one dense product per V-cycle; coarsest
                                            levels up to 16384 unknowns) (TN_COARSE_PCG) */
+    int      transfer;                  /* multigrid transfers and GCA interpolation: TN_TRANSFER_CONSTANT (the
+                                           application's, stokes_solver.hpp:150-151) or TN_TRANSFER_LINEAR
+                                           (tn_prolongate_linear_add / tn_restrict_linear, GCA with
+                                           InterpolationMode::Linear) (TN_TRANSFER_CONSTANT) */
 } tn_solver_options;
 #define TN_SMOOTHER_CHEBYSHEV 0
 #define TN_SMOOTHER_JACOBI 1

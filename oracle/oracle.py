@@ -56,6 +56,7 @@ def lib():
         L.tno_prolongate_add.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
         L.tno_restrict.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
         L.tno_gca_coarsen.argtypes = [ctypes.c_void_p, dp, dp]
+        L.tno_gca_coarsen_w.argtypes = [ctypes.c_void_p, dp, dp, dp]
         L.tno_masked_dot.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dpp, dpp]
         L.tno_masked_dot.restype = ctypes.c_double
         L.tno_epsdivdiv_vjp_logeta.argtypes = [ctypes.c_void_p, dpp, dpp, dp]
@@ -251,15 +252,117 @@ def null_space_modes(shell: Shell):
     return modes
 
 
-def gca_coarsen(fine_op: EpsDivDiv, fine_mats=None):
-    """Two-grid GCA (gca.hpp) of a Neumann fine operator or stored fine matrices."""
+def gca_coarsen(fine_op: EpsDivDiv, fine_mats=None, linear=False):
+    """Two-grid GCA (gca.hpp) of a Neumann fine operator or stored fine matrices; InterpolationMode::Linear
+    (the linear-transfer weights of the fine level) when linear, else Constant."""
     sh = fine_op.shell
     nlc, nrc = (sh.nl + 1) // 2, (sh.nr + 1) // 2
     out = np.zeros((10, nlc - 1, nlc - 1, nrc - 1, 2, 18, 18))
     s = fine_op._struct(False)
     fm = None if fine_mats is None else _dp(np.ascontiguousarray(fine_mats))
-    lib().tno_gca_coarsen(ctypes.byref(s), fm, _dp(out))
+    lw = _dp(np.ascontiguousarray(linear_weights(sh))) if linear else None
+    lib().tno_gca_coarsen_w(ctypes.byref(s), fm, lw, _dp(out))
     return out
+
+
+def _linear_parents(x, y, r, nrf):
+    """Coarse parents of a fine node for the linear transfers (prolongation_linear.hpp operator())."""
+    if x % 2 == 0 and y % 2 == 0 and r % 2 == 0:
+        return 0, (x // 2, y // 2), (x // 2, y // 2), r // 2, r // 2
+    rb = r // 2 if r < nrf - 1 else r // 2 - 1
+    if x % 2 == 0 and y % 2 == 0:
+        return 1, (x // 2, y // 2), (x // 2, y // 2), rb, rb + 1
+    if x % 2 == 0:
+        return 2, (x // 2, y // 2), (x // 2, y // 2 + 1), rb, rb + 1
+    if y % 2 == 0:
+        return 2, (x // 2, y // 2), (x // 2 + 1, y // 2), rb, rb + 1
+    return 2, (x // 2 + 1, y // 2), (x // 2, y // 2 + 1), rb, rb + 1
+
+
+_LINW_CACHE: dict = {}
+
+
+def linear_weights(fine: Shell):
+    """(10, nl, nl, nr, 2) weights of prolongation_linear_weights (grid_transfer_linear.hpp:13-157) per fine
+    node: (1 - nu, nu) for radially aligned nodes, (0.5 (1 - nu), 0.5 nu) for nodes on a facet, nu measured
+    along the radius from the (chord midpoint of the) bottom coarse pair to the top pair; (1, 0) on coarse
+    nodes."""
+    key = (fine.lat_level, fine.rad_level, fine.r_min, fine.r_max)
+    if key in _LINW_CACHE:
+        return _LINW_CACHE[key]
+    nl, nr = fine.nl, fine.nr
+    w = np.zeros((10, nl, nl, nr, 2))
+    w[..., 0] = 1.0
+    C, R = fine.coords, fine.radii
+    for d in range(10):
+        for x in range(nl):
+            for y in range(nl):
+                for r in range(nr):
+                    kind, p0, p1, rb, rt = _linear_parents(x, y, r, nr)
+                    if kind == 0:
+                        continue
+                    nf = np.linalg.norm(C[d, x, y] * R[r])
+                    if kind == 1:
+                        nb = np.linalg.norm(C[d, x, y] * R[2 * rb])
+                        nt = np.linalg.norm(C[d, x, y] * R[2 * rt])
+                    else:
+                        u0, u1 = C[d, 2 * p0[0], 2 * p0[1]], C[d, 2 * p1[0], 2 * p1[1]]
+                        nb = np.linalg.norm(0.5 * (u0 * R[2 * rb] + u1 * R[2 * rb]))
+                        nt = np.linalg.norm(0.5 * (u0 * R[2 * rt] + u1 * R[2 * rt]))
+                    nu = (nf - nb) / (nt - nb)
+                    w[d, x, y, r] = (1.0 - nu, nu) if kind == 1 else (0.5 * (1.0 - nu), 0.5 * nu)
+    _LINW_CACHE[key] = w
+    return w
+
+
+def prolongate_linear_add(fine: Shell, coarse_v, fine_v):
+    """fine_v += P coarse_v with the linear prolongation per component (ProlongationLinear)."""
+    w = linear_weights(fine)
+    nr = fine.nr
+    out = np.array(fine_v, dtype=np.float64, copy=True)
+    for d in range(10):
+        for x in range(fine.nl):
+            for y in range(fine.nl):
+                for r in range(nr):
+                    kind, p0, p1, rb, rt = _linear_parents(x, y, r, nr)
+                    for c in range(coarse_v.shape[0]):
+                        cv = coarse_v[c, d]
+                        if kind == 0:
+                            v = cv[p0[0], p0[1], rb]
+                        elif kind == 1:
+                            v = w[d, x, y, r, 0] * cv[p0[0], p0[1], rb] + w[d, x, y, r, 1] * cv[p0[0], p0[1], rt]
+                        else:
+                            v = (w[d, x, y, r, 0] * (cv[p0[0], p0[1], rb] + cv[p1[0], p1[1], rb]) +
+                                 w[d, x, y, r, 1] * (cv[p0[0], p0[1], rt] + cv[p1[0], p1[1], rt]))
+                        out[c, d, x, y, r] += v
+    return out
+
+
+def restrict_linear(fine: Shell, fine_v):
+    """P^T over owned fine nodes, then the coarse interface sum (RestrictionLinear per component)."""
+    w = linear_weights(fine)
+    coarse = fine.coarser()
+    nr = fine.nr
+    out = np.zeros((fine_v.shape[0],) + coarse.scalar_shape)
+    for d in range(10):
+        for x in range(fine.nl):
+            for y in range(fine.nl):
+                if not fine.owned_lat[d, x, y]:
+                    continue
+                for r in range(nr):
+                    kind, p0, p1, rb, rt = _linear_parents(x, y, r, nr)
+                    for c in range(fine_v.shape[0]):
+                        f = fine_v[c, d, x, y, r]
+                        if kind == 0:
+                            out[c, d, p0[0], p0[1], rb] += f
+                        elif kind == 1:
+                            out[c, d, p0[0], p0[1], rb] += w[d, x, y, r, 0] * f
+                            out[c, d, p0[0], p0[1], rt] += w[d, x, y, r, 1] * f
+                        else:
+                            for p in (p0, p1):
+                                out[c, d, p[0], p[1], rb] += w[d, x, y, r, 0] * f
+                                out[c, d, p[0], p[1], rt] += w[d, x, y, r, 1] * f
+    return coarse.interface_sum(out)
 
 
 class Divergence:
@@ -521,11 +624,14 @@ def pcg(A, x, b, dot, max_iter, rtol, atol=1e-16, precond=None, history=None):
 
 
 class Multigrid:
-    """V-cycle (multigrid.hpp:216-432); levels[0] is the coarsest."""
+    """V-cycle (multigrid.hpp:216-432); levels[0] is the coarsest. transfer: "constant" (the application's
+    ProlongationVecConstant / RestrictionVecConstant) or "linear" (ProlongationLinear / RestrictionLinear per
+    component)."""
 
-    def __init__(self, ops, shells, smoothers, coarse_solve, num_cycles=1):
+    def __init__(self, ops, shells, smoothers, coarse_solve, num_cycles=1, transfer="constant"):
         self.ops, self.shells, self.smoothers = ops, shells, smoothers
         self.coarse_solve, self.num_cycles = coarse_solve, num_cycles
+        self.transfer = transfer
 
     def _rec(self, level, x, b):
         if level == 0:
@@ -533,10 +639,14 @@ class Multigrid:
         A = self.ops[level]
         x = self.smoothers[level].solve(A, x, b)
         res = b - A(x)
-        rc = restrict(self.shells[level], res)
+        lin = self.transfer == "linear"
+        rc = restrict_linear(self.shells[level], res) if lin else restrict(self.shells[level], res)
         ec = np.zeros_like(rc)
         ec = self._rec(level - 1, ec, rc)
-        prolongate_add(self.shells[level], ec, x)
+        if lin:
+            x = prolongate_linear_add(self.shells[level], ec, x)
+        else:
+            prolongate_add(self.shells[level], ec, x)
         x = self.smoothers[level].solve(A, x, b)
         return x
 
@@ -675,7 +785,8 @@ class VelocityHierarchy:
     the diagonal mode, and Chebyshev smoothers with given lambda_max values."""
 
     def __init__(self, fine: Shell, k, bc_cmb, bc_surface, num_levels, gca=True, lambdas=None, cheb_order=2,
-                 cheb_iters=2, coarse_max_iter=50, coarse_rtol=1e-6, coarse_atol=1e-16):
+                 cheb_iters=2, coarse_max_iter=50, coarse_rtol=1e-6, coarse_atol=1e-16, transfer="constant"):
+        self.transfer = transfer
         shells = [fine]
         for _ in range(num_levels - 1):
             shells.insert(0, shells[0].coarser())
@@ -686,12 +797,13 @@ class VelocityHierarchy:
         kk = k
         for l in range(num_levels - 2, -1, -1):
             if gca:
+                lin = transfer == "linear"
                 if l == num_levels - 2:
                     src = EpsDivDiv(shells[l + 1], k=k, bc_cmb=NEUMANN, bc_surface=NEUMANN)
-                    m = gca_coarsen(src)
+                    m = gca_coarsen(src, linear=lin)
                 else:
                     src = EpsDivDiv(shells[l + 1], k=np.ones(shells[l + 1].scalar_shape), stored=self.mats[l + 1])
-                    m = gca_coarsen(src, fine_mats=self.mats[l + 1])
+                    m = gca_coarsen(src, fine_mats=self.mats[l + 1], linear=lin)
                 self.mats[l] = m
                 ops[l] = EpsDivDiv(shells[l], k=np.ones(shells[l].scalar_shape), bc_cmb=bc_cmb, bc_surface=bc_surface,
                                    stored=m)
@@ -720,7 +832,7 @@ class VelocityHierarchy:
         ops = [(lambda v, l=l: self.apply(l, v)) for l in range(n)]
         it, rtol, atol = self.coarse
         coarse = lambda A, x, b: pcg(A, x, b, self.shells[0].dot, it, rtol, atol)
-        return Multigrid(ops, self.shells, smoothers, coarse, num_cycles)
+        return Multigrid(ops, self.shells, smoothers, coarse, num_cycles, transfer=self.transfer)
 
 
 class StokesSystem:

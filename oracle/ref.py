@@ -66,7 +66,9 @@ def lib(threads: int = 0):
         L.tnr_vector_mass.argtypes = [I, D, D, dp, dp]
         L.tnr_prolongate_add.argtypes = [I, D, D, dp, dp]
         L.tnr_restrict.argtypes = [I, D, D, dp, dp]
-        L.tnr_gca.argtypes = [I, I, D, D, dp, dp]
+        L.tnr_gca.argtypes = [I, I, D, D, dp, I, dp]
+        L.tnr_prolongate_linear_add.argtypes = [I, D, D, I, dp, dp]
+        L.tnr_restrict_linear.argtypes = [I, D, D, I, dp, dp]
         L.tnr_stokes_create.argtypes = [I, I, D, D, I, I, dp, dpp, dp, dpp, I, I, I, I, I, I,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(D)]
         L.tnr_stokes_solve.argtypes = [ctypes.c_void_p, D, D, I, dp, dp, dp, I, ctypes.POINTER(I), ctypes.POINTER(D)]
@@ -180,12 +182,32 @@ def restrict(fine_lat, fine_v, r_min=0.55, r_max=1.0):
     return out
 
 
-def gca(fine_lat, coarse_lat, k, r_min=0.55, r_max=1.0):
-    """Element matrices of level coarse_lat from TwoGridGCA chained down from the Neumann operator of fine_lat."""
+def gca(fine_lat, coarse_lat, k, linear=False, r_min=0.55, r_max=1.0):
+    """Element matrices of level coarse_lat from TwoGridGCA chained down from the Neumann operator of fine_lat
+    (InterpolationMode::Linear when linear, else Constant)."""
     nc = _sizes(coarse_lat)
     out = np.zeros((10, nc - 1, nc - 1, nc - 1, 2, 18, 18))
     L = lib()
-    _check(L, L.tnr_gca(fine_lat, coarse_lat, r_min, r_max, _dp(_c(k)), _dp(out)))
+    _check(L, L.tnr_gca(fine_lat, coarse_lat, r_min, r_max, _dp(_c(k)), int(linear), _dp(out)))
+    return out
+
+
+def prolongate_linear_add(fine_lat, coarse_v, fine_v, r_min=0.55, r_max=1.0):
+    """fine += P coarse with ProlongationLinear per component."""
+    out = _c(fine_v).copy()
+    cv = _c(coarse_v)
+    L = lib()
+    _check(L, L.tnr_prolongate_linear_add(fine_lat, r_min, r_max, cv.shape[0], _dp(cv), _dp(out)))
+    return out
+
+
+def restrict_linear(fine_lat, fine_v, r_min=0.55, r_max=1.0):
+    """coarse = R fine with RestrictionLinear per component (interface sum included)."""
+    fv = _c(fine_v)
+    nc = _sizes(fine_lat - 1)
+    out = np.zeros((fv.shape[0], 10, nc, nc, nc))
+    L = lib()
+    _check(L, L.tnr_restrict_linear(fine_lat, r_min, r_max, fv.shape[0], _dp(fv), _dp(out)))
     return out
 
 

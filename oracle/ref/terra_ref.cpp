@@ -59,6 +59,8 @@ void randomize( VectorQ1Vec< double, 3 >& v );
 #include "terra/fe/wedge/operators/shell/gradient_kerngen.hpp"
 #include "terra/fe/wedge/operators/shell/kmass.hpp"
 #include "terra/fe/wedge/operators/shell/prolongation_constant.hpp"
+#include "terra/fe/wedge/operators/shell/prolongation_linear.hpp"
+#include "terra/fe/wedge/operators/shell/restriction_linear.hpp"
 #include "terra/fe/wedge/operators/shell/restriction_constant.hpp"
 #include "terra/fe/wedge/operators/shell/vector_mass.hpp"
 #include "terra/grid/bit_masks.hpp"
@@ -435,10 +437,47 @@ int tnr_restrict( int fine_lat, double r_min, double r_max, const double* fine, 
     } );
 }
 
+/// Linear transfers per component (ProlongationLinear in Add mode, prolongation_linear.hpp:14-194;
+/// RestrictionLinear with its interface sum, restriction_linear.hpp:16-215); ncomp components, each a
+/// contiguous nodal field.
+int tnr_prolongate_linear_add( int fine_lat, double r_min, double r_max, int ncomp, const double* coarse, double* fine )
+{
+    return guarded( [&] {
+        Level& F = level( fine_lat, fine_lat, r_min, r_max );
+        Level& C = level( fine_lat - 1, fine_lat - 1, r_min, r_max );
+        fe::wedge::operators::shell::ProlongationLinear< double > P( F.coords, F.radii, linalg::OperatorApplyMode::Add );
+        for ( int c = 0; c < ncomp; ++c )
+        {
+            VectorQ1Scalar< double > cv( "c", *C.domain, C.owned ), fv( "f", *F.domain, F.owned );
+            load( cv.grid_data(), coarse + c * C.nodes() );
+            load( fv.grid_data(), fine + c * F.nodes() );
+            linalg::apply( P, cv, fv );
+            store( fv.grid_data(), fine + c * F.nodes() );
+        }
+    } );
+}
+
+int tnr_restrict_linear( int fine_lat, double r_min, double r_max, int ncomp, const double* fine, double* coarse )
+{
+    return guarded( [&] {
+        Level& F = level( fine_lat, fine_lat, r_min, r_max );
+        Level& C = level( fine_lat - 1, fine_lat - 1, r_min, r_max );
+        fe::wedge::operators::shell::RestrictionLinear< double > R( *C.domain, F.coords, F.radii );
+        for ( int c = 0; c < ncomp; ++c )
+        {
+            VectorQ1Scalar< double > fv( "f", *F.domain, F.owned ), cv( "c", *C.domain, C.owned );
+            load( fv.grid_data(), fine + c * F.nodes() );
+            linalg::apply( R, fv, cv );
+            store( cv.grid_data(), coarse + c * C.nodes() );
+        }
+    } );
+}
+
 /// Galerkin coarse operators built top-down as the application does (stokes_solver.hpp:375-389): the Neumann
 /// operator of level fine_lat with nodal coefficient k, coarsened by TwoGridGCA level by level down to
-/// coarse_lat. out receives the element matrices of level coarse_lat.
-int tnr_gca( int fine_lat, int coarse_lat, double r_min, double r_max, const double* k, double* out )
+/// coarse_lat, with InterpolationMode::Linear when linear != 0 (else Constant, the application's default). out
+/// receives the element matrices of level coarse_lat.
+int tnr_gca( int fine_lat, int coarse_lat, double r_min, double r_max, const double* k, int linear, double* out )
 {
     return guarded( [&] {
         if ( coarse_lat >= fine_lat || coarse_lat < 0 )
@@ -463,7 +502,8 @@ int tnr_gca( int fine_lat, int coarse_lat, double r_min, double r_max, const dou
         for ( int i = n - 2; i >= 0; --i )
         {
             linalg::solvers::TwoGridGCA< double, Viscous >(
-                i == n - 2 ? A_fine : A_c[i + 1], A_c[i], i, elements.grid_data() );
+                i == n - 2 ? A_fine : A_c[i + 1], A_c[i], i, elements.grid_data(), true,
+                linear ? linalg::solvers::InterpolationMode::Linear : linalg::solvers::InterpolationMode::Constant );
         }
         const int nc = L0.nl - 1, rc = L0.nr - 1;
         long      o  = 0;

@@ -1176,6 +1176,13 @@ int tno_restrict(int llf, int rlf, int ncomp, const double* const* fine, double*
 
 int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coarse_mats)
 {
+    return tno_gca_coarsen_w(fine_op, fine_mats, NULL, coarse_mats);
+}
+
+/* linw: per fine node the two linear-transfer weights (InterpolationMode::Linear, gca.hpp:231-243, :327-342),
+ * or NULL for the constant mode. */
+int tno_gca_coarsen_w(const tno_op* fine_op, const double* fine_mats, const double* linw, double* coarse_mats)
+{
     const int nlf = fine_op->nl, nrf = fine_op->nr, nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
     static const int shifts[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1198,10 +1205,16 @@ int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coar
                                     continue;
                                 }
                                 int rb = ir < nrf - 1 ? ir / 2 : ir / 2 - 1, rt = rb + 1;
+                                double lw0 = 0.5, lw1 = 0.5;
+                                if (linw) {
+                                    long fi = IDX4(nlf, nrf, d, ix, iy, ir);
+                                    lw0 = linw[2 * fi];
+                                    lw1 = linw[2 * fi + 1];
+                                }
                                 if (ix % 2 == 0 && iy % 2 == 0) {
-                                    if (fl == 2 || fl == 5) { P[fl][2] = 0.5; P[fl][5] = 0.5; }
-                                    else if (fl == 0 || fl == 3) { P[fl][0] = 0.5; P[fl][3] = 0.5; }
-                                    else { P[fl][1] = 0.5; P[fl][4] = 0.5; }
+                                    if (fl == 2 || fl == 5) { P[fl][2] = lw0; P[fl][5] = lw1; }
+                                    else if (fl == 0 || fl == 3) { P[fl][0] = lw0; P[fl][3] = lw1; }
+                                    else { P[fl][1] = lw0; P[fl][4] = lw1; }
                                     continue;
                                 }
                                 int x0, x1, y0, y1, cl[4];
@@ -1214,6 +1227,13 @@ int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coar
                                 } else {
                                     x0 = ix / 2 + 1; x1 = ix / 2; y0 = iy / 2; y1 = iy / 2 + 1;
                                     cl[0] = 1; cl[1] = 2; cl[2] = 4; cl[3] = 5;
+                                }
+                                if (linw) {
+                                    P[fl][cl[0]] = lw0;
+                                    P[fl][cl[1]] = lw0;
+                                    P[fl][cl[2]] = lw1;
+                                    P[fl][cl[3]] = lw1;
+                                    continue;
                                 }
                                 P[fl][cl[0]] = pweight(ix, iy, ir, x0, y0, rb);
                                 P[fl][cl[1]] = pweight(ix, iy, ir, x1, y1, rb);

@@ -77,6 +77,7 @@ int tno_restrict(int lat_level_f, int rad_level_f, int ncomp, const double* cons
  * operator's on-the-fly local matrices from `fine_op` (Neumann) are used. Output
  * (10, nlc-1, nlc-1, nrc-1, 2, 18, 18). */
 int tno_gca_coarsen(const tno_op* fine_op, const double* fine_mats, double* coarse_mats);
+int tno_gca_coarsen_w(const tno_op* fine_op, const double* fine_mats, const double* linw, double* coarse_mats);
 
 /* owned-masked dot of ncomp-component nodal vectors. */
 double tno_masked_dot(int lat_level, int nr, int ncomp, const double* const* a, const double* const* b);

@@ -114,6 +114,8 @@ tn::MgOptions mg_options(const tn_solver_options& o)
     m.smoother        = o.smoother;
     m.jacobi_omega    = o.jacobi_omega;
     m.coarse_dense    = o.coarse_solver == TN_COARSE_DENSE ? 1 : 0;
+    m.transfer        = o.transfer == TN_TRANSFER_LINEAR ? 1 : 0;
+    need(o.transfer == TN_TRANSFER_CONSTANT || o.transfer == TN_TRANSFER_LINEAR, "unknown transfer");
     need(o.coarse_solver == TN_COARSE_PCG || o.coarse_solver == TN_COARSE_DENSE, "unknown coarse solver");
     need(o.gca == 0 || o.gca == 1, "gca must be 0 or 1");
     need(o.smoother == TN_SMOOTHER_CHEBYSHEV || o.smoother == TN_SMOOTHER_JACOBI, "unknown smoother");
@@ -539,6 +541,45 @@ int tn_prolongate_add(tn_shell* shell, int fine_level, int precision, int ncomp,
     });
 }
 
+int tn_prolongate_linear_add(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* coarse_dev,
+                             void* const* fine_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell && coarse_dev && fine_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        need(fine_level >= 1, "fine level needs a coarser level");
+        const auto& L  = shell->impl->level(fine_level);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            return tn::prolongate_linear_add<T>(L.nl(), L.nr(), ncomp, L.linear_weights<T>(as_stream(stream)),
+                                                reinterpret_cast<const T* const*>(coarse_dev),
+                                                reinterpret_cast<T* const*>(fine_dev), as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "prolongation launch failed");
+    });
+}
+
+int tn_restrict_linear(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
+                       void* const* coarse_dev, void* stream)
+{
+    return guarded([&] {
+        need(shell && coarse_dev && fine_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        need(fine_level >= 1, "fine level needs a coarser level");
+        const auto& L  = shell->impl->level(fine_level);
+        const auto& Lc = shell->impl->level(fine_level - 1);
+        const int   rc = dispatch_prec(precision, [&](auto t) {
+            using T = decltype(t);
+            auto c  = reinterpret_cast<T* const*>(coarse_dev);
+            int  r  = tn::restrict_linear_owned<T>(L.nl(), L.nr(), ncomp, L.owned_lat.as<uint8_t>(),
+                                                 L.linear_weights<T>(as_stream(stream)),
+                                                 reinterpret_cast<const T* const*>(fine_dev), c, as_stream(stream));
+            return r ? r : tn::interface_sum<T>(Lc.iface, Lc.nr(), ncomp, c, as_stream(stream));
+        });
+        if (rc) throw tn::Error(tn::kErrCuda, "restriction launch failed");
+    });
+}
+
 int tn_restrict(tn_shell* shell, int fine_level, int precision, int ncomp, const void* const* fine_dev,
                 void* const* coarse_dev, void* stream)
 {
@@ -789,9 +830,15 @@ int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream)
 
 int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream)
 {
+    return tn_gca_build_interpolated(fine, coarse, TN_TRANSFER_CONSTANT, stream);
+}
+
+int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, void* stream)
+{
     return guarded([&] {
         need(fine && coarse, "NULL operator");
-        tn::gca_coarsen(*as_edd(fine), *as_edd(coarse), as_stream(stream));
+        need(interpolation == TN_TRANSFER_CONSTANT || interpolation == TN_TRANSFER_LINEAR, "unknown interpolation");
+        tn::gca_coarsen(*as_edd(fine), *as_edd(coarse), as_stream(stream), interpolation == TN_TRANSFER_LINEAR);
         tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
     });
 }
@@ -847,6 +894,7 @@ void tn_solver_options_default(tn_solver_options* o)
     o->smoother                  = TN_SMOOTHER_CHEBYSHEV;
     o->jacobi_omega              = 1.0;
     o->coarse_solver             = TN_COARSE_PCG;
+    o->transfer                  = TN_TRANSFER_CONSTANT;
 }
 
 int tn_stokes_solver_create(tn_shell* shell, int velocity_level, const double* eta_nodal_dev,

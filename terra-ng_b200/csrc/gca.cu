@@ -71,8 +71,10 @@ __device__ __forceinline__ double pweight(int xf, int yf, int rf, int xc, int yc
 }
 
 // Interpolation matrix P[fine node][coarse node] of fine wedge (fx, fy, fr, w)
-// (gca.hpp:204-383, InterpolationMode::Constant).
-__device__ void interp_matrix(int fx, int fy, int fr, int w, int nrf, double (&P)[6][6])
+// (gca.hpp:204-383): InterpolationMode::Constant, or InterpolationMode::Linear when linw (the fine level's
+// linear-transfer weights, two per node: prolongation_linear_weights) is given.
+__device__ void interp_matrix(int d, int fx, int fy, int fr, int w, int nlf, int nrf, const double* linw,
+                              double (&P)[6][6])
 {
     for (int a = 0; a < 6; ++a)
         for (int b = 0; b < 6; ++b) P[a][b] = 0.0;
@@ -83,10 +85,16 @@ __device__ void interp_matrix(int fx, int fy, int fr, int w, int nrf, double (&P
             continue;
         }
         const int rb = ir < nrf - 1 ? ir / 2 : ir / 2 - 1, rt = rb + 1;
+        double    lw0 = 0.0, lw1 = 0.0;
+        if (linw) {
+            const int64_t fi = node_index(nlf, nrf, d, ix, iy, ir);
+            lw0              = linw[2 * fi];
+            lw1              = linw[2 * fi + 1];
+        }
         if (ix % 2 == 0 && iy % 2 == 0) {
             const int a = fl % 3;  // lateral index of the fine node == coarse node
-            P[fl][a]     = 0.5;
-            P[fl][a + 3] = 0.5;
+            P[fl][a]     = linw ? lw0 : 0.5;
+            P[fl][a + 3] = linw ? lw1 : 0.5;
             continue;
         }
         int x0, x1, y0, y1, c0, c1, c2, c3;
@@ -99,6 +107,13 @@ __device__ void interp_matrix(int fx, int fy, int fr, int w, int nrf, double (&P
         } else {
             x0 = ix / 2 + 1, x1 = ix / 2, y0 = iy / 2, y1 = iy / 2 + 1;
             c0 = 1, c1 = 2, c2 = 4, c3 = 5;
+        }
+        if (linw) {
+            P[fl][c0] = lw0;
+            P[fl][c1] = lw0;
+            P[fl][c2] = lw1;
+            P[fl][c3] = lw1;
+            continue;
         }
         P[fl][c0] = pweight(ix, iy, ir, x0, y0, rb);
         P[fl][c1] = pweight(ix, iy, ir, x1, y1, rb);
@@ -123,6 +138,7 @@ struct GcaBuildArgs {
     const double* kq0;            // fine cell coefficient or nullptr
     const double* fine_mats;      // stored fine matrices [342][fine cells] or nullptr
     double*       out;            // coarse matrices [342][coarse cells]
+    const double* linw = nullptr; // fine linear-transfer weights (linear interpolation) or nullptr (constant)
 };
 
 // Fine wedge matrix of (d, fx, fy, fr, w) into Af (dimension-wise ordering),
@@ -206,7 +222,7 @@ __global__ void __launch_bounds__(kN * kN) gca_build_kernel(GcaBuildArgs A)
         const int fx = 2 * xc + (h & 1), fy = 2 * yc + ((h >> 1) & 1), fr = 2 * rc + ((h >> 2) & 1);
         for (int w = 0; w < 2; ++w) {
             load_fine_matrix(A, d, fx, fy, fr, w, Af, G, kwJ);
-            if (tid == 0) interp_matrix(fx, fy, fr, w, nrf, P);
+            if (tid == 0) interp_matrix(d, fx, fy, fr, w, nlf, nrf, A.linw, P);
             __syncthreads();
             // Y = A P_vec: P_vec couples equal dimensions only
             double y = 0.0;
@@ -501,9 +517,9 @@ inline dim3 cell_grid(int nl, int nr, int thr) { return dim3((nr - 1 + thr - 1) 
 int gca_values_per_cell() { return 2 * kPack; }
 
 int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
-              const double* fine_mats, double* coarse_mats, cudaStream_t st)
+              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights)
 {
-    GcaBuildArgs a{nlf, nrf, coords_f, radii_f, k_f, kq0_f, fine_mats, coarse_mats};
+    GcaBuildArgs a{nlf, nrf, coords_f, radii_f, k_f, kq0_f, fine_mats, coarse_mats, linear_weights};
     const int    nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
     const int    ncc = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
     gca_build_kernel<<<ncc, kN * kN, 0, st>>>(a);

@@ -86,6 +86,37 @@ std::unique_ptr<Shell> make_shell(int lat_level, int rad_level, int num_levels, 
     return sh;
 }
 
+template <>
+const double* DeviceLevel::linear_weights<double>(cudaStream_t st) const
+{
+    if (linw64.get() == nullptr) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cuda_check(cudaStreamIsCapturing(st, &cap), "capture status");
+        if (cap != cudaStreamCaptureStatusNone)
+            throw Error(kErrState, "linear-transfer weights must be built before stream capture");
+        DevBuf w(sizeof(double) * 2 * static_cast<size_t>(nodes()));
+        if (linear_transfer_weights(nl(), nr(), coords64.as<double>(), radii64.as<double>(), w.as<double>(), st) != 0)
+            throw Error(kErrCuda, "linear-transfer weight launch failed");
+        cuda_check(cudaStreamSynchronize(st), "linear-transfer weights");
+        linw64 = std::move(w);
+    }
+    return linw64.as<double>();
+}
+
+template <>
+const float* DeviceLevel::linear_weights<float>(cudaStream_t st) const
+{
+    if (linw32.get() == nullptr) {
+        const double* w64 = linear_weights<double>(st);
+        DevBuf        w(sizeof(float) * 2 * static_cast<size_t>(nodes()));
+        if (convert_f64_to_f32(2 * nodes(), w64, w.as<float>(), st) != 0)
+            throw Error(kErrCuda, "conversion launch failed");
+        cuda_check(cudaStreamSynchronize(st), "linear-transfer weights");
+        linw32 = std::move(w);
+    }
+    return linw32.as<float>();
+}
+
 template <typename T>
 void zero_components(int64_t n, int ncomp, T* const* v, cudaStream_t st)
 {
@@ -148,7 +179,7 @@ void EpsDivDivOp::ensure_baked(bool need32, cudaStream_t st)
     }
 }
 
-void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st)
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear)
 {
     if (fine.shell != coarse.shell || coarse.level != fine.level - 1)
         throw Error(kErrArg, "GCA needs operators on consecutive levels of one shell");
@@ -158,8 +189,9 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st)
     coarse.mats.alloc(static_cast<size_t>(coarse.mats_values()) * sizeof(double));
     const double* kf   = (!fine.stored && !fine.q0) ? fine.k.as<double>() : nullptr;
     const double* kq0f = (!fine.stored && fine.q0) ? fine.k.as<double>() : nullptr;
+    const double* linw = linear ? Lf.linear_weights<double>(st) : nullptr;
     if (gca_build(Lf.nl(), Lf.nr(), Lf.coords<double>(), Lf.radii<double>(), kf, kq0f,
-                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st) != 0)
+                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st, linw) != 0)
         throw Error(kErrCuda, "GCA build launch failed");
     coarse.stored        = true;
     coarse.baked_bc[0]   = -1;

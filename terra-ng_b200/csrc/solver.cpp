@@ -142,7 +142,7 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     if (fine.precision != 0) throw Error(kErrArg, "the multigrid hierarchy is built from an FP64 operator");
     if (fine_ < 1) throw Error(kErrArg, "multigrid needs at least two levels");
     if (o.cheb_order < 1 || o.cheb_iters < 0 || o.num_vcycles < 1 || o.coarse_max_iter < 0 ||
-        (o.smoother != 0 && o.smoother != 1) || !(o.jacobi_omega > 0.0))
+        (o.smoother != 0 && o.smoother != 1) || !(o.jacobi_omega > 0.0) || (o.transfer != 0 && o.transfer != 1))
         throw Error(kErrArg, "invalid multigrid options");
     const int nlev = fine_ + 1;
     ops64_.resize(nlev);
@@ -175,7 +175,7 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     for (int l = fine_ - 1; l >= 0; --l) {
         auto op = make_op(l);
         if (o.gca) {
-            gca_coarsen(*ops64_[l + 1], *op, st);
+            gca_coarsen(*ops64_[l + 1], *op, st, o.transfer == 1);
         } else {
             const DeviceLevel& Lc = sh->level(l);
             const auto&        kf = ops64_[l + 1]->k;
@@ -205,6 +205,11 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     }
 
     if (o.coarse_dense) build_dense_coarse(st);
+    if (o.transfer == 1)  // linear-transfer weights of every fine level, before any stream capture
+        for (int l = 1; l <= fine_; ++l) {
+            sh->level(l).linear_weights<double>(st);
+            if (o.fp32) sh->level(l).linear_weights<float>(st);
+        }
 
     // FP32 operators where the apply is matrix-free
     if (o.fp32) {
@@ -459,13 +464,21 @@ void VelocityMultigrid::vcycle(int l, T* x, const T* b, cudaStream_t st)
     T*            ec = W.e[l - 1].data();
     const T*      fin[3]  = {res, res + sf, res + 2 * sf};
     T*            cout[3] = {rc, rc + sc, rc + 2 * sc};
-    chk(restrict_owned<T>(L.nl(), L.nr(), 3, L.owned_lat.as<uint8_t>(), fin, cout, st), "restrict");
+    if (opt_.transfer == 1)
+        chk(restrict_linear_owned<T>(L.nl(), L.nr(), 3, L.owned_lat.as<uint8_t>(), L.linear_weights<T>(st), fin,
+                                     cout, st),
+            "restrict");
+    else
+        chk(restrict_owned<T>(L.nl(), L.nr(), 3, L.owned_lat.as<uint8_t>(), fin, cout, st), "restrict");
     chk(interface_sum<T>(Lc.iface, Lc.nr(), 3, cout, st), "interface sum");
     cuda_check(cudaMemsetAsync(ec, 0, sizeof(T) * W.e[l - 1].total(), st), "zero correction");
     vcycle<T>(l - 1, ec, rc, st);
     const T* cin[3]  = {ec, ec + sc, ec + 2 * sc};
     T*       fout[3] = {x, x + sf, x + 2 * sf};
-    chk(prolongate_add<T>(L.nl(), L.nr(), 3, cin, fout, st), "prolongate");
+    if (opt_.transfer == 1)
+        chk(prolongate_linear_add<T>(L.nl(), L.nr(), 3, L.linear_weights<T>(st), cin, fout, st), "prolongate");
+    else
+        chk(prolongate_add<T>(L.nl(), L.nr(), 3, cin, fout, st), "prolongate");
     smooth<T>(l, x, b, st);
 }
 

@@ -102,6 +102,17 @@ template <typename T>
 int restrict_owned(int nlf, int nrf, int ncomp, const uint8_t* owned_lat_fine, const T* const* fine, T* const* coarse,
                    cudaStream_t stream);
 
+// Linear transfers (transfer_linear.cu): w holds two weights per fine node (linear_transfer_weights, FP64
+// from the fine coordinates; FP32 copies for the FP32 V-cycle).
+int linear_transfer_weights(int nlf, int nrf, const double* coords_fine, const double* radii_fine, double* w,
+                            cudaStream_t stream);
+template <typename T>
+int prolongate_linear_add(int nlf, int nrf, int ncomp, const T* w, const T* const* coarse, T* const* fine,
+                          cudaStream_t stream);
+template <typename T>
+int restrict_linear_owned(int nlf, int nrf, int ncomp, const uint8_t* owned_lat_fine, const T* w,
+                          const T* const* fine, T* const* coarse, cudaStream_t stream);
+
 // ----------------------------------------------------------------------------
 // Interface sum over diamond-edge duplicates (vector_ops.cu).
 // classes: offsets (num_classes + 1) into members (lateral indices).
@@ -148,8 +159,9 @@ int convert_f32_to_f64(int64_t n, const float* in, double* out, cudaStream_t str
 int gca_values_per_cell();
 // coarse = sum P^T A_f P (fine level nlf, nrf); A_f from the nodal / cell
 // coefficient (on-the-fly element matrices) or from stored fine matrices.
+// linear_weights: the fine level's linear-transfer weights for InterpolationMode::Linear, or nullptr (Constant)
 int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
-              const double* fine_mats, double* coarse_mats, cudaStream_t st);
+              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights = nullptr);
 // element matrices of a level (the stored form of the on-the-fly operator)
 int element_matrices(int nl, int nr, const double* coords, const double* radii, const double* k, const double* kq0,
                      double* mats, cudaStream_t st);

@@ -112,6 +112,10 @@ struct DeviceLevel {
     DevBuf     dup_offset, dup_members;
     DevBuf     canon_lat;  // (10, nl, nl) int32: lowest lateral index of the node's duplicate class
     IfaceTable iface;
+    // linear-transfer weights of this level as the fine level (2 per node), built on first use
+    mutable DevBuf linw64, linw32;
+    template <typename T>
+    const T* linear_weights(cudaStream_t st) const;
 
     int     nl() const { return host.nl; }
     int     nr() const { return host.nr; }
@@ -166,6 +170,11 @@ inline const float* DeviceLevel::radii<float>() const
 {
     return radii32.as<float>();
 }
+
+template <>
+const double* DeviceLevel::linear_weights<double>(cudaStream_t st) const;
+template <>
+const float* DeviceLevel::linear_weights<float>(cudaStream_t st) const;
 
 struct Shell {
     std::vector<std::unique_ptr<DeviceLevel>> levels;  // 0 = coarsest
@@ -244,7 +253,8 @@ struct EpsDivDivOp : Operator {
 };
 // TwoGridGCA (gca.hpp:41-531): coarse.mats = sum P^T A_fine P with A_fine the
 // fine operator's stored matrices or its on-the-fly Neumann element matrices.
-void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st);
+// linear: InterpolationMode::Linear (the fine level's linear-transfer weights) instead of Constant.
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear = false);
 
 // B (DivergenceKerngen): velocity level -> pressure level (level - 1).
 struct DivergenceOp : Operator {

@@ -54,6 +54,7 @@ struct MgOptions {
     int      smoother     = 0;    // 0: Chebyshev (cheb_order, cheb_iters), 1: damped Jacobi (cheb_iters steps)
     double   jacobi_omega = 1.0;  // Jacobi relaxation
     int      coarse_dense = 0;    // 0: coarsest CG (the reference's PCG); 1: dense inverse built once, exact solve
+    int      transfer     = 0;    // 0: constant transfers (the application's), 1: linear (also in the GCA build)
 };
 
 // Velocity multigrid (Multigrid, multigrid.hpp:216-432) over levels 0..fine of

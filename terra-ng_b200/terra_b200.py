@@ -29,6 +29,7 @@ STORED_OFF, STORED_FULL = 0, 1
 
 SMOOTHER_CHEBYSHEV, SMOOTHER_JACOBI = 0, 1
 COARSE_PCG, COARSE_DENSE = 0, 1
+TRANSFER_CONSTANT, TRANSFER_LINEAR = 0, 1
 
 
 class SolverOptions(ctypes.Structure):
@@ -55,6 +56,7 @@ class SolverOptions(ctypes.Structure):
         ("smoother", ctypes.c_int),
         ("jacobi_omega", ctypes.c_double),
         ("coarse_solver", ctypes.c_int),
+        ("transfer", ctypes.c_int),
     ]
 
 
@@ -105,6 +107,9 @@ def load(path: str = LIB_PATH):
         "tn_vector_mass_apply": ([vp, i, i, vpp, vpp, vp], i),
         "tn_prolongate_add": ([vp, i, i, i, vpp, vpp, vp], i),
         "tn_restrict": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_prolongate_linear_add": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_restrict_linear": ([vp, i, i, i, vpp, vpp, vp], i),
+        "tn_gca_build_interpolated": ([vp, vp, i, vp], i),
         "tn_interface_sum": ([vp, i, i, i, vpp, vp], i),
         "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
         "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
@@ -387,9 +392,9 @@ class EpsDivDiv(Operator):
         return out
 
 
-def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None):
-    """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build)."""
-    _check(load().tn_gca_build(fine._h, coarse._h, _stream(stream)))
+def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None, interpolation=0):
+    """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build / tn_gca_build_interpolated)."""
+    _check(load().tn_gca_build_interpolated(fine._h, coarse._h, interpolation, _stream(stream)))
 
 
 def random_vector(shell: Shell, level: int, ncomp: int, seed: int, dtype=None, stream=None):
@@ -558,6 +563,20 @@ def stokes_rhs_enforce(shell: Shell, level: int, u, bc_cmb: int, bc_surface: int
     _check(load().tn_stokes_rhs_enforce(shell.handle, level % shell.num_levels, _prec(cu[0].dtype), bc_cmb,
                                         bc_surface, _ptrs(cu), _stream(stream)))
     return u
+
+
+def prolongate_linear_add(shell: Shell, fine_level: int, coarse, fine, stream=None):
+    cc, cf = _comps(coarse), _comps(fine)
+    _check(load().tn_prolongate_linear_add(shell.handle, fine_level % shell.num_levels, _prec(cc[0].dtype), len(cc),
+                                           _ptrs(cc), _ptrs(cf), _stream(stream)))
+    return fine
+
+
+def restrict_linear(shell: Shell, fine_level: int, fine, coarse, stream=None):
+    cf, cc = _comps(fine), _comps(coarse)
+    _check(load().tn_restrict_linear(shell.handle, fine_level % shell.num_levels, _prec(cf[0].dtype), len(cf),
+                                     _ptrs(cf), _ptrs(cc), _stream(stream)))
+    return coarse
 
 
 def solver_options(**kw) -> SolverOptions:

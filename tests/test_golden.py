@@ -109,6 +109,10 @@ def test_oracle_gca_and_rhs_equal_reference():
     sh, u, p = inp["shell"], inp["u"], inp["p"]
     m = O.gca_coarsen(O.EpsDivDiv(sh, k=inp["k"], bc_cmb=O.NEUMANN, bc_surface=O.NEUMANN))
     assert rel_err(m[0], g["gca_d0"]) < TOL
+    ml = O.gca_coarsen(O.EpsDivDiv(sh, k=inp["k"], bc_cmb=O.NEUMANN, bc_surface=O.NEUMANN), linear=True)
+    assert rel_err(ml[0], g["gca_linear_d0"]) < TOL
+    assert rel_err(O.prolongate_linear_add(sh, inp["u_coarse"], u), g["prolong_linear_add"]) < TOL
+    assert rel_err(O.restrict_linear(sh, u), g["restrict_linear"]) < TOL
     ref_sums = g["gca_sumsq"]
     assert abs((m * m).sum() - ref_sums[0]) <= 1e-12 * ref_sums[0]
     for bc in ((1, 2), (2, 1), (1, 1)):

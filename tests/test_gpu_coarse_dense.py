@@ -117,3 +117,30 @@ def test_stokes_dense_coarse_reaches_tolerance(cuda):
         out[name] = (np.stack([x[c].cpu().numpy() for c in range(3)]), its)
     assert rel_err(out["dense"][0], out["pcg"][0]) < 1e-6
     assert out["dense"][1] <= out["pcg"][1]
+
+
+@pytest.mark.parametrize("gca", [1, 0])
+def test_vcycle_linear_transfers_match_oracle(cuda, gca):
+    """One V-cycle with the linear transfers (and, with GCA, linear interpolation in the Galerkin build),
+    against the oracle's V-cycle with the same transfers and an exact coarsest solve."""
+    import torch
+
+    level, nlev, bcs = 4, 3, (1, 2)
+    sh = O.Shell(level)
+    k = smooth_viscosity(sh, 33, 100.0)
+    g = T.Shell(level, num_levels=nlev)
+    solver = T.VelocitySolver(g, eta=_t(k), bc_cmb=bcs[0], bc_surface=bcs[1], gca=gca,
+                              coarse_solver=T.COARSE_DENSE, transfer=T.TRANSFER_LINEAR)
+    lambdas = [None] + [solver.level_lambda(l) for l in range(1, nlev)]
+    o = solver.options
+    H = O.VelocityHierarchy(sh, k, bcs[0], bcs[1], nlev, gca=bool(gca), lambdas=lambdas,
+                            cheb_order=o.chebyshev_order, cheb_iters=o.chebyshev_iterations, coarse_rtol=1e-14,
+                            coarse_max_iter=5000, transfer="linear")
+    if gca:
+        for l in range(nlev - 1):
+            assert rel_err(solver.level_matrices(l), H.mats[l]) < 1e-12
+    b = O.enforce_rhs_bcs(sh, consistent(sh, O.seeded_normal(sh.vec_shape, 34)), *bcs)
+    ref = H.multigrid().solve(np.zeros(sh.vec_shape), b)
+    x = torch.zeros(sh.vec_shape, dtype=torch.float64, device=cuda)
+    solver.vcycle(x, _t(b))
+    assert rel_err(x.cpu().numpy(), ref) < 1e-9

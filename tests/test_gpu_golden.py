@@ -98,6 +98,17 @@ def test_gca_and_rhs_match_reference(cuda):
     m = coarse.local_matrices()
     assert rel_err(m[0], g["gca_d0"]) < TOL64
     assert abs((m * m).sum() - g["gca_sumsq"][0]) <= 1e-12 * g["gca_sumsq"][0]
+    T.gca_build(fine, coarse, interpolation=T.TRANSFER_LINEAR)
+    assert rel_err(coarse.local_matrices()[0], g["gca_linear_d0"]) < TOL64
+    import torch
+
+    uu = _t(inp["u"], cuda)
+    fine_v = uu.clone()
+    T.prolongate_linear_add(gs, 1, _t(inp["u_coarse"], cuda), fine_v)
+    assert rel_err(_np(fine_v), g["prolong_linear_add"]) < TOL64
+    cv = torch.zeros((3,) + inp["shell"].coarser().scalar_shape, dtype=torch.float64, device=cuda)
+    T.restrict_linear(gs, 1, uu, cv)
+    assert rel_err(_np(cv), g["restrict_linear"]) < TOL64
     u = inp["u"]
     for bc in ((1, 2), (2, 1), (1, 1)):
         v = _t(u, cuda)

@@ -12,7 +12,9 @@ degree <= 4 (10^2 contrast); buoyancy right-hand side from a seeded
 temperature field (harmonics plus N(0, 0.01) noise). FGMRES(30) with the
 block-triangular preconditioner (Schur = inverse lumped 1/eta pressure mass,
 velocity = one GMG V(2,2) Chebyshev(2) cycle, Galerkin coarse operators,
-coarsest CG 50 iterations / 1e-6), relative tolerance 1e-8 with constant
+coarsest level 2 solved directly with its inverse formed once at set-up
+(--coarse dense; --coarse pcg: the reference's 50-iteration / 1e-6 CG, the
+other one is timed once beside it)), relative tolerance 1e-8 with constant
 pressure treated as a null vector (see the solver's project_pressure_mean).
 
 One step = one solve from a zero initial guess. value = seconds per solve of
@@ -58,7 +60,7 @@ FP64_ITERATIONS = 357
 WORKLOAD = ("L6 Stokes solve (10x65x65x65 velocity nodes, pressure on L5, hierarchy L2..L6), no-slip CMB / "
             "free-slip surface, 1e2 viscosity contrast from 8 seeded SH (l<=4) x radial cosine, seeded buoyancy "
             "RHS; FGMRES(30) + block-triangular GMG V(2,2) Chebyshev(2) preconditioner, GCA coarse operators, "
-            "rtol 1e-8")
+            "FP64 coarsest solve on L2, rtol 1e-8")
 
 
 def _args():
@@ -68,6 +70,10 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--coarse", default="dense", choices=["dense", "pcg"],
+                    help="coarsest-level solve of the timed solvers: dense (the assembled level-2 operator inverted "
+                         "once, an exact solve per V-cycle) or pcg (the reference's 50-iteration CG); the other "
+                         "one is timed once beside it")
     ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "coupling",
                                                              "precondition", "adjoint-L5", "solve-L7"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
@@ -428,13 +434,16 @@ def run_ours(a):
     temp = S.temperature(shell, fine, seed=SEED_TEMP)
     f = S.buoyancy_rhs(shell, fine, temp, *BCS)
     nlp, nrp = shell.dims(fine - 1)
+    coarse = {"dense": T.COARSE_DENSE, "pcg": T.COARSE_PCG}
+    other = "pcg" if a.coarse == "dense" else "dense"
     opts = dict(bc_cmb=BCS[0], bc_surface=BCS[1], relative_tolerance=1e-8, absolute_tolerance=0.0,
                 max_iterations=3000, restart=30, project_pressure_mean=1, normalize_pressure=1)
     solvers, setup_s = {}, {}
     for name, mixed in (("mixed", 1), ("fp64", 0)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        solvers[name] = T.StokesSolver(shell, eta=eta, mixed_precision=mixed, **opts)
+        solvers[name] = T.StokesSolver(shell, eta=eta, mixed_precision=mixed, coarse_solver=coarse[a.coarse],
+                                       **opts)
         torch.cuda.synchronize()
         setup_s[name] = time.perf_counter() - t0
 
@@ -474,6 +483,17 @@ def run_ours(a):
     if ws > 1:
         torch.distributed.barrier()
     ck = clocks.stop()
+    # the other coarsest-level solve, timed once after one warm-up solve
+    alt = {}
+    for name, mixed in (("mixed", 1), ("fp64", 0)):
+        s_alt = T.StokesSolver(shell, eta=eta, mixed_precision=mixed, coarse_solver=coarse[other], **opts)
+        for t in x:
+            t.zero_()
+        s_alt.solve(x, b)
+        dt_alt, _ = _timed(torch, lambda: ([t.zero_() for t in x], s_alt.solve(x, b)))
+        its_alt, rr_alt, conv_alt = s_alt.result()
+        alt[name] = {"s": dt_alt, "iterations": its_alt, "relative_residual": rr_alt, "converged": conv_alt}
+        del s_alt
     t_mixed = results["mixed"]["s"]
     t_tensor = torch.tensor([t_mixed, results["fp64"]["s"]], device=dev, dtype=torch.float64)
     if ws > 1:
@@ -536,6 +556,7 @@ def run_ours(a):
                                                   "level-5 Galerkin matrices streamed per V-cycle)",
                        "replicas": ws, "velocity_dofs": dofs_u},
             "fp64_solve_s": t_fp64, "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "coarse_solver": a.coarse, f"coarse_{other}": alt,
             "iterations": {"mixed": results["mixed"]["iterations"], "fp64": results["fp64"]["iterations"]},
             "relative_residual": {k: results[k]["relres"] for k in results},
             "relative_residual_without_projection": {k: results[k]["full_relres"] for k in results},

@@ -75,10 +75,11 @@ def _args():
                          "once, an exact solve per V-cycle) or pcg (the reference's 50-iteration CG); the other "
                          "one is timed once beside it")
     ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "coupling",
-                                                             "precondition", "adjoint-L5", "solve-L7"],
+                                                             "precondition", "adjoint-L5", "solve-L7", "gca-build"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
                          "apply; coupling: the L6 B and B^T applies (FP64); precondition: one application of the "
-                         "L6 mixed-precision block preconditioner; adjoint-L5: the L5 misfit gradient with a "
+                         "L6 mixed-precision block preconditioner; gca-build: the Galerkin coarse operators of the "
+                         "L6 hierarchy on the FP64 tensor cores and as scalar FMAs; adjoint-L5: the L5 misfit gradient with a "
                          "finite-difference check; solve-L7: the L7 mixed and FP64 solves plus one adjoint "
                          "gradient")
     return ap.parse_args()
@@ -378,6 +379,43 @@ def run_coupling(a):
                                    "algorithmic_bytes": bytes_b,
                                    "divergence_frac": bytes_b / tb / 1e9 / peak,
                                    "gradient_frac": bytes_b / tg / 1e9 / peak}}), flush=True)
+
+
+def run_gca_build(a):
+    """TwoGridGCA down the level-6 hierarchy (Neumann L6 operator -> L5 -> L4 -> L3 -> L2): the batched 18 x 18
+    triple products on the FP64 tensor cores (mma m8n8k4) against the same kernel structure with scalar FMAs."""
+    import numpy as np
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    fine = NUM_LEVELS - 1
+    eta = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA), device="cuda")
+    ops = {fine: T.EpsDivDiv(shell, fine, k=eta, bc_cmb=0, bc_surface=0)}
+    for l in range(fine - 1, -1, -1):
+        nl, nr = shell.dims(l)
+        ops[l] = T.EpsDivDiv(shell, l, k=torch.ones((10, nl, nl, nr), dtype=torch.float64, device="cuda"),
+                             bc_cmb=0, bc_surface=0)
+    times, mats = {}, {}
+    for tc in (True, False):
+        per = []
+        for l in range(fine - 1, -1, -1):
+            T.gca_build(ops[l + 1], ops[l], tensor_cores=tc)  # warm-up (also the input of the next level)
+            dt, _ = _timed(torch, lambda: T.gca_build(ops[l + 1], ops[l], tensor_cores=tc))
+            per.append({"coarse_level": l + (LEVEL - fine), "ms": dt * 1e3})
+        times["tensor_cores" if tc else "scalar"] = per
+        mats[tc] = ops[0].local_matrices()
+    diff = float(np.abs(mats[True] - mats[False]).max() / np.abs(mats[False]).max())
+    tot = {k: sum(p["ms"] for p in v) for k, v in times.items()}
+    print(json.dumps({"metric": "L6 GCA hierarchy build time", "value": tot["tensor_cores"], "unit": "ms",
+                      "n_gpus": 1, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "TwoGridGCA chain of the L6 hierarchy (Neumann L6 operator with the "
+                                             "benchmark viscosity, coarse levels 5..2)"},
+                      "per_level": times, "scalar_total_ms": tot["scalar"],
+                      "speedup_tensor_cores": tot["scalar"] / tot["tensor_cores"],
+                      "level2_max_rel_diff_tensor_vs_scalar": diff}), flush=True)
 
 
 def run_precondition(a):
@@ -856,6 +894,8 @@ def main():
         run_coupling(a)
     elif a.workload == "precondition":
         run_precondition(a)
+    elif a.workload == "gca-build":
+        run_gca_build(a)
     elif a.workload == "adjoint-L5":
         run_adjoint_l5(a)
     elif a.workload == "solve-L7":

@@ -290,8 +290,11 @@ int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream);
 /* TwoGridGCA with its interpolation_mode argument (gca.hpp:72-78):
  * TN_TRANSFER_CONSTANT (InterpolationMode::Constant, tn_gca_build) or
  * TN_TRANSFER_LINEAR (InterpolationMode::Linear: P from the linear-transfer
- * weights, gca.hpp:231-243, :327-342). Synchronous. */
-int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, void* stream);
+ * weights, gca.hpp:231-243, :327-342). tensor_cores = 1 runs the batched 18 x 18
+ * triple products P^T A P on the FP64 tensor cores (the default of tn_gca_build
+ * and of the solvers), 0 as scalar FMAs. Synchronous. */
+int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, int tensor_cores,
+                              void* stream);
 /* get_local_matrix for every cell: host array (10, nl-1, nl-1, nr-1, 2, 18, 18),
  * dimension-wise ordering (row = node + 6 * component), without boundary
  * treatment. Synchronous. */
@@ -410,6 +413,25 @@ int tn_stokes_misfit_gradient(tn_solver* solver, const double* const* x_dev, con
 /* stored matrices of coarse level 0..fine-1 of the hierarchy, layout as
  * tn_operator_copy_local_matrices. */
 int tn_solver_level_matrices(tn_solver* solver, int level, double* mats_host);
+
+/* ---- XDMF output that doubles as a checkpoint ------------------------------
+ * The file format of the reference's XDMFOutput (src/terra/io/xdmf.hpp:13-148,
+ * :293-512, :898-1060): per write, `<name>_<step>.bin` for every field and
+ * `step_<step>.xmf`; the first write also writes geometry.bin (physical node
+ * coordinates, 4- or 8-byte floats), topology.bin (two int64 wedges per hex
+ * cell), checkpoint_metadata.bin and a README into `directory` (created if
+ * missing). Binary order per diamond: r, y, x (fastest), component. A writer
+ * covers one level of a shell; fields (1 or 3 components, device data in
+ * `precision`, written with output_bytes = 4 or 8) are added before the first
+ * write and read at every write. Synchronous. tn_xdmf_read restores a field of
+ * step `step` into device memory (read_xdmf_checkpoint_grid). */
+typedef struct tn_xdmf tn_xdmf;
+int  tn_xdmf_create(tn_shell* shell, int level, const char* directory, int geometry_bytes, tn_xdmf** out);
+int  tn_xdmf_add(tn_xdmf* x, const char* name, int precision, int ncomp, void* const* comps_dev, int output_bytes);
+int  tn_xdmf_write(tn_xdmf* x, void* stream);
+void tn_xdmf_destroy(tn_xdmf* x);
+int  tn_xdmf_read(tn_shell* shell, int level, const char* directory, const char* name, int step, int precision,
+                  int ncomp, void* const* comps_dev);
 
 #ifdef __cplusplus
 }

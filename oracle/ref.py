@@ -76,6 +76,7 @@ def lib(threads: int = 0):
         L.tnr_stokes_destroy.restype = None
         L.tnr_epsdivdiv_time.argtypes = [I, D, D, dp, I, I, dp, I, dp]
         L.tnr_rhs_enforce.argtypes = [I, D, D, I, I, dp]
+        L.tnr_xdmf_write.argtypes = [I, D, D, ctypes.c_char_p, I, dp, dp, I]
         _check(L, L.tnr_init(int(threads) if threads > 0 else (os.cpu_count() or 1)))
         _lib = L
     return _lib
@@ -209,6 +210,13 @@ def restrict_linear(fine_lat, fine_v, r_min=0.55, r_max=1.0):
     L = lib()
     _check(L, L.tnr_restrict_linear(fine_lat, r_min, r_max, fv.shape[0], _dp(fv), _dp(out)))
     return out
+
+
+def xdmf_write(lat, directory, scalar, vec, geometry_bytes=4, out_bytes=4, r_min=0.55, r_max=1.0):
+    """The reference's XDMFOutput: one step with the scalar field "temperature" and the vector "velocity"."""
+    L = lib()
+    _check(L, L.tnr_xdmf_write(lat, r_min, r_max, directory.encode(), geometry_bytes, _dp(_c(scalar)), _dp(_c(vec)),
+                               out_bytes))
 
 
 def rhs_enforce(lat, f, bc_cmb, bc_surface, r_min=0.55, r_max=1.0):

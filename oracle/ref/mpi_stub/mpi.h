@@ -3,8 +3,8 @@
  * The container has no MPI. On one rank every MPI call the reference's Stokes path makes is either a
  * no-op or a copy: reductions and gathers copy the send buffer into the receive buffer (MPI_IN_PLACE
  * leaves it), point-to-point calls never fire because same-rank interface pairs are direct copies
- * (communication_plan.hpp), and size/rank are 1/0. Datatypes encode their element size. MPI-IO is not
- * provided (the checker never writes XDMF). */
+ * (communication_plan.hpp), and size/rank are 1/0. Datatypes encode their element size. MPI-IO maps onto stdio
+ * (one process writes the whole file). */
 #ifndef TN_REF_MPI_STUB_H
 #define TN_REF_MPI_STUB_H
 
@@ -177,6 +177,56 @@ static inline int MPI_Type_create_hindexed(int, const int*, const MPI_Aint*, MPI
 static inline int MPI_Type_commit(MPI_Datatype*) { return MPI_SUCCESS; }
 static inline int MPI_Type_free(MPI_Datatype*) { return MPI_SUCCESS; }
 static inline double MPI_Wtime() { return 0.0; }
+
+/* MPI-IO on one rank: a small table of stdio handles (the reference's XDMF writer and checkpoint reader) */
+#include <stdio.h>
+struct tn_mpi_files_ {
+    FILE* f[64];
+};
+static inline tn_mpi_files_& tn_mpi_files() { static tn_mpi_files_ t = {}; return t; }
+static inline int MPI_File_open(MPI_Comm, const char* path, int amode, MPI_Info, MPI_File* fh)
+{
+    FILE* f = 0;
+    if (amode & MPI_MODE_RDONLY) f = fopen(path, "rb");
+    else {
+        f = fopen(path, "r+b");
+        if (!f && (amode & MPI_MODE_CREATE)) f = fopen(path, "w+b");
+    }
+    if (!f) return MPI_ERR_OTHER;
+    for (int i = 1; i < 64; ++i)
+        if (!tn_mpi_files().f[i]) { tn_mpi_files().f[i] = f; *fh = i; return MPI_SUCCESS; }
+    fclose(f);
+    return MPI_ERR_OTHER;
+}
+static inline int MPI_File_close(MPI_File* fh)
+{
+    if (*fh > 0 && *fh < 64 && tn_mpi_files().f[*fh]) { fclose(tn_mpi_files().f[*fh]); tn_mpi_files().f[*fh] = 0; }
+    *fh = 0;
+    return MPI_SUCCESS;
+}
+static inline int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype, MPI_Datatype, const char*, MPI_Info)
+{
+    return fseek(tn_mpi_files().f[fh], (long) disp, SEEK_SET) == 0 ? MPI_SUCCESS : MPI_ERR_OTHER;
+}
+static inline int MPI_File_write_all(MPI_File fh, const void* buf, int count, MPI_Datatype t, MPI_Status*)
+{
+    size_t n = (size_t) count * (size_t) t;
+    return fwrite(buf, 1, n, tn_mpi_files().f[fh]) == n ? MPI_SUCCESS : MPI_ERR_OTHER;
+}
+static inline int MPI_File_read_all(MPI_File fh, void* buf, int count, MPI_Datatype t, MPI_Status*)
+{
+    size_t n = (size_t) count * (size_t) t;
+    return fread(buf, 1, n, tn_mpi_files().f[fh]) == n ? MPI_SUCCESS : MPI_ERR_OTHER;
+}
+static inline int MPI_File_get_size(MPI_File fh, MPI_Offset* size)
+{
+    FILE* f = tn_mpi_files().f[fh];
+    long  p = ftell(f);
+    fseek(f, 0, SEEK_END);
+    *size = ftell(f);
+    fseek(f, p, SEEK_SET);
+    return MPI_SUCCESS;
+}
 
 #ifdef __cplusplus
 }

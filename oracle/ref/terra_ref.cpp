@@ -64,6 +64,7 @@ void randomize( VectorQ1Vec< double, 3 >& v );
 #include "terra/fe/wedge/operators/shell/restriction_constant.hpp"
 #include "terra/fe/wedge/operators/shell/vector_mass.hpp"
 #include "terra/grid/bit_masks.hpp"
+#include "terra/io/xdmf.hpp"
 #include "terra/grid/grid_types.hpp"
 #include "terra/grid/shell/bit_masks.hpp"
 #include "terra/grid/shell/spherical_shell.hpp"
@@ -767,6 +768,28 @@ int tnr_rhs_enforce( int lat, double r_min, double r_max, int bc_cmb, int bc_sur
         Kokkos::fence();
         store( fv.block_1().grid_data(), f );
         store( fv.block_2().grid_data(), f + 3 * nu );
+    } );
+}
+
+/// The reference's XDMFOutput (io/xdmf.hpp) on level lat: one write() of a scalar field and a 3-vector field (FP64
+/// data written with out_bytes 4 or 8), geometry in geometry_bytes, into `directory`.
+int tnr_xdmf_write( int lat, double r_min, double r_max, const char* directory, int geometry_bytes, const double* scalar,
+                    const double* vec, int out_bytes )
+{
+    return guarded( [&] {
+        Level& L = level( lat, lat, r_min, r_max );
+        using X  = io::XDMFOutput< double >;
+        X xdmf( directory, *L.domain, L.coords, L.radii,
+                geometry_bytes == 8 ? X::OutputTypeFloat::Float64 : X::OutputTypeFloat::Float32 );
+        const auto ot = out_bytes == 8 ? X::OutputTypeFloat::Float64 : X::OutputTypeFloat::Float32;
+        Grid4DDataScalar< double > s( std::string( "temperature" ), size_t( 10 ), size_t( L.nl ), size_t( L.nl ),
+                                      size_t( L.nr ) );
+        load( s, scalar );
+        Grid4DDataVec< double, 3 > v( "velocity", 10, L.nl, L.nl, L.nr );
+        load( v, vec );
+        xdmf.add( s, ot );
+        xdmf.add( v, ot );
+        xdmf.write();
     } );
 }
 

@@ -13,6 +13,10 @@ struct tn_shell {
 struct tn_operator {
     std::unique_ptr<tn::Operator> op;
 };
+struct tn_xdmf {
+    tn::Xdmf* impl = nullptr;
+    ~tn_xdmf() { tn::xdmf_destroy(impl); }
+};
 struct tn_solver {
     tn_shell*                           shell = nullptr;
     std::unique_ptr<tn::StokesSolver>   stokes;
@@ -830,15 +834,17 @@ int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream)
 
 int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream)
 {
-    return tn_gca_build_interpolated(fine, coarse, TN_TRANSFER_CONSTANT, stream);
+    return tn_gca_build_interpolated(fine, coarse, TN_TRANSFER_CONSTANT, 1, stream);
 }
 
-int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, void* stream)
+int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, int tensor_cores,
+                              void* stream)
 {
     return guarded([&] {
         need(fine && coarse, "NULL operator");
         need(interpolation == TN_TRANSFER_CONSTANT || interpolation == TN_TRANSFER_LINEAR, "unknown interpolation");
-        tn::gca_coarsen(*as_edd(fine), *as_edd(coarse), as_stream(stream), interpolation == TN_TRANSFER_LINEAR);
+        tn::gca_coarsen(*as_edd(fine), *as_edd(coarse), as_stream(stream), interpolation == TN_TRANSFER_LINEAR,
+                        tensor_cores != 0);
         tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
     });
 }
@@ -1143,3 +1149,48 @@ namespace tn {
 Shell* shell_of(tn_shell* s) { return s ? s->impl.get() : nullptr; }
 void   set_last_error(const std::string& message) { g_last_error = message; }
 }  // namespace tn
+
+extern "C" {
+
+/* ---- XDMF output / checkpoint ------------------------------------------- */
+int tn_xdmf_create(tn_shell* shell, int level, const char* directory, int geometry_bytes, tn_xdmf** out)
+{
+    return guarded([&] {
+        need(shell && directory && out, "NULL argument");
+        auto x  = std::make_unique<tn_xdmf>();
+        x->impl = tn::xdmf_create(shell->impl.get(), level, directory, geometry_bytes);
+        *out    = x.release();
+    });
+}
+
+int tn_xdmf_add(tn_xdmf* x, const char* name, int precision, int ncomp, void* const* comps_dev, int output_bytes)
+{
+    return guarded([&] {
+        need(x && name && comps_dev, "NULL argument");
+        tn::xdmf_add(x->impl, name, precision, ncomp, comps_dev, output_bytes);
+    });
+}
+
+int tn_xdmf_write(tn_xdmf* x, void* stream)
+{
+    return guarded([&] {
+        need(x != nullptr, "NULL argument");
+        tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "synchronize");
+        tn::xdmf_write(x->impl);
+    });
+}
+
+void tn_xdmf_destroy(tn_xdmf* x) { delete x; }
+
+int tn_xdmf_read(tn_shell* shell, int level, const char* directory, const char* name, int step, int precision,
+                 int ncomp, void* const* comps_dev)
+{
+    return guarded([&] {
+        need(shell && directory && name && comps_dev, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 3, "ncomp must be 1..3");
+        precision_size(precision);
+        tn::xdmf_read(shell->impl.get(), level, directory, name, step, precision, ncomp, comps_dev);
+    });
+}
+
+}  // extern "C"

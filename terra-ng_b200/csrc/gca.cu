@@ -147,10 +147,11 @@ struct GcaBuildArgs {
 __device__ void load_fine_matrix(const GcaBuildArgs& A, int d, int fx, int fy, int fr, int w, double (&Af)[kN][kN],
                                  double (&G)[6][3], double& kwJ)
 {
-    const int nlf = A.nlf, nrf = A.nrf;
-    const int tid = threadIdx.x;
-    const int i = tid / kN, j = tid % kN;
-    const int ni = i % 6, di = i / 6, nj = j % 6, dj = j / 6;
+    const int  nlf = A.nlf, nrf = A.nrf;
+    const int  tid = threadIdx.x;
+    const bool ent = tid < kN * kN;  // threads beyond the 324 entries only take part in the barrier
+    const int  i = ent ? tid / kN : 0, j = ent ? tid % kN : 0;
+    const int  ni = i % 6, di = i / 6, nj = j % 6, dj = j / 6;
     if (A.fine_mats == nullptr) {
         // element matrix: gradients and k|det J| first
         if (tid == 0) {
@@ -185,8 +186,8 @@ __device__ void load_fine_matrix(const GcaBuildArgs& A, int d, int fx, int fy, i
         __syncthreads();
         // A(i,j) = kwJ [delta_{di dj} g_i.g_j + g_i[dj] g_j[di] - 2/3 g_i[di] g_j[dj]]
         const double gij = (di == dj) ? (G[ni][0] * G[nj][0] + G[ni][1] * G[nj][1] + G[ni][2] * G[nj][2]) : 0.0;
-        Af[i][j]         = kwJ * (gij + G[ni][dj] * G[nj][di] - (2.0 / 3.0) * G[ni][di] * G[nj][dj]);
-    } else {
+        if (ent) Af[i][j] = kwJ * (gij + G[ni][dj] * G[nj][di] - (2.0 / 3.0) * G[ni][di] * G[nj][dj]);
+    } else if (ent) {
         const int     ncf = 10 * (nlf - 1) * (nlf - 1) * (nrf - 1);
         const int64_t fc  = node_index(nlf - 1, nrf - 1, d, fx, fy, fr);
         Af[i][j]          = A.fine_mats[static_cast<int64_t>(w * kPack + pidx(i, j)) * ncf + fc];
@@ -241,6 +242,95 @@ __global__ void __launch_bounds__(kN * kN) gca_build_kernel(GcaBuildArgs A)
     if (i <= j) {
         A.out[static_cast<int64_t>(0 * kPack + pidx(i, j)) * ncc + cell] = acc0;
         A.out[static_cast<int64_t>(1 * kPack + pidx(i, j)) * ncc + cell] = acc1;
+    }
+}
+
+// The same triple products on the FP64 tensor cores (mma.sync m8n8k4, f64 in and out). P_vec = I_3 (x) P
+// couples equal dimensions only, so A_c += P_vec^T A_f P_vec splits into nine 6 x 6 blocks
+// A_c[di][dj] += P^T A_f[di][dj] P. Warp b of the first nine owns block b = (di, dj) for both coarse wedges
+// and keeps it in two 8 x 8 accumulator fragments (the 6 x 6 blocks and P zero-padded to 8 x 8); per fine
+// wedge it runs Y = A_f[di][dj] P (two k = 4 steps) and A_c += P^T Y (two more), staging Y through shared
+// memory to turn the accumulator layout into the B-operand layout. The 324 threads of the first eleven warps
+// assemble the fine element matrix as in gca_build_kernel.
+constexpr int kMmaWarps   = 11;  // 352 threads: 324 matrix entries, warps 0-8 for the nine blocks
+constexpr int kMmaThreads = 32 * kMmaWarps;
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kMmaThreads) gca_build_mma_kernel(GcaBuildArgs A)
+{
+    const int nlf = A.nlf, nrf = A.nrf;
+    const int nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
+    const int ncc  = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
+    const int cell = blockIdx.x;
+    if (cell >= ncc) return;
+    const int rc = cell % (nrc - 1);
+    int       t  = cell / (nrc - 1);
+    const int yc = t % (nlc - 1);
+    t /= (nlc - 1);
+    const int xc = t % (nlc - 1);
+    const int d  = t / (nlc - 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int b = warp < 9 ? warp : 0, bdi = b / 3, bdj = b % 3;  // block (di, dj) of this warp
+    const int fr_row = lane >> 2, fr_col = lane & 3;             // fragment coordinates (PTX m8n8k4 f64)
+
+    __shared__ double Af[kN][kN];
+    __shared__ double P[6][6];
+    __shared__ double G[6][3];
+    __shared__ double kwJ;
+    __shared__ double Yb[9][8][8];
+
+    double acc0[2] = {0.0, 0.0}, acc1[2] = {0.0, 0.0};  // coarse wedges 0 and 1
+    for (int h = 0; h < 8; ++h) {
+        const int fx = 2 * xc + (h & 1), fy = 2 * yc + ((h >> 1) & 1), fr = 2 * rc + ((h >> 2) & 1);
+        for (int w = 0; w < 2; ++w) {
+            load_fine_matrix(A, d, fx, fy, fr, w, Af, G, kwJ);
+            if (tid == 0) interp_matrix(d, fx, fy, fr, w, nlf, nrf, A.linw, P);
+            __syncthreads();
+            if (warp < 9) {
+                // Y = A_f[di][dj] (rows 6 di.., cols 6 dj..) x P, k = 0..7 in two steps
+                double y[2] = {0.0, 0.0};
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
+                    const int k  = ks * 4 + fr_col;
+                    const double a  = (fr_row < 6 && k < 6) ? Af[6 * bdi + fr_row][6 * bdj + k] : 0.0;
+                    const double bb = (k < 6 && fr_row < 6) ? P[k][fr_row] : 0.0;  // B[k][col = lane >> 2]
+                    dmma_8x8x4(y, a, bb);
+                }
+                Yb[b][fr_row][2 * fr_col]     = y[0];
+                Yb[b][fr_row][2 * fr_col + 1] = y[1];
+                __syncwarp();
+                const bool to0 = target_wedge(h, w) == 0;
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
+                    const int    k  = ks * 4 + fr_col;
+                    const double a  = (fr_row < 6 && k < 6) ? P[k][fr_row] : 0.0;  // (P^T)[row][k]
+                    const double bb = Yb[b][k][fr_row];                          // Y[k][col = lane >> 2]
+                    if (to0)
+                        dmma_8x8x4(acc0, a, bb);
+                    else
+                        dmma_8x8x4(acc1, a, bb);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (warp < 9) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int r = fr_row, c = 2 * fr_col + e;
+            if (r >= 6 || c >= 6) continue;
+            const int i = 6 * bdi + r, j = 6 * bdj + c;
+            if (i > j) continue;
+            A.out[static_cast<int64_t>(0 * kPack + pidx(i, j)) * ncc + cell] = acc0[e];
+            A.out[static_cast<int64_t>(1 * kPack + pidx(i, j)) * ncc + cell] = acc1[e];
+        }
     }
 }
 
@@ -517,12 +607,16 @@ inline dim3 cell_grid(int nl, int nr, int thr) { return dim3((nr - 1 + thr - 1) 
 int gca_values_per_cell() { return 2 * kPack; }
 
 int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
-              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights)
+              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights,
+              bool tensor_cores)
 {
     GcaBuildArgs a{nlf, nrf, coords_f, radii_f, k_f, kq0_f, fine_mats, coarse_mats, linear_weights};
     const int    nlc = (nlf + 1) / 2, nrc = (nrf + 1) / 2;
     const int    ncc = 10 * (nlc - 1) * (nlc - 1) * (nrc - 1);
-    gca_build_kernel<<<ncc, kN * kN, 0, st>>>(a);
+    if (tensor_cores)
+        gca_build_mma_kernel<<<ncc, kMmaThreads, 0, st>>>(a);
+    else
+        gca_build_kernel<<<ncc, kN * kN, 0, st>>>(a);
     return launch_status();
 }
 

@@ -179,7 +179,7 @@ void EpsDivDivOp::ensure_baked(bool need32, cudaStream_t st)
     }
 }
 
-void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear)
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear, bool tensor_cores)
 {
     if (fine.shell != coarse.shell || coarse.level != fine.level - 1)
         throw Error(kErrArg, "GCA needs operators on consecutive levels of one shell");
@@ -191,7 +191,7 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, 
     const double* kq0f = (!fine.stored && fine.q0) ? fine.k.as<double>() : nullptr;
     const double* linw = linear ? Lf.linear_weights<double>(st) : nullptr;
     if (gca_build(Lf.nl(), Lf.nr(), Lf.coords<double>(), Lf.radii<double>(), kf, kq0f,
-                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st, linw) != 0)
+                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st, linw, tensor_cores) != 0)
         throw Error(kErrCuda, "GCA build launch failed");
     coarse.stored        = true;
     coarse.baked_bc[0]   = -1;

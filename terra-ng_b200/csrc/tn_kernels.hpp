@@ -159,9 +159,11 @@ int convert_f32_to_f64(int64_t n, const float* in, double* out, cudaStream_t str
 int gca_values_per_cell();
 // coarse = sum P^T A_f P (fine level nlf, nrf); A_f from the nodal / cell
 // coefficient (on-the-fly element matrices) or from stored fine matrices.
-// linear_weights: the fine level's linear-transfer weights for InterpolationMode::Linear, or nullptr (Constant)
+// linear_weights: the fine level's linear-transfer weights for InterpolationMode::Linear, or nullptr (Constant);
+// tensor_cores: the triple products as FP64 tensor-core tiles (mma m8n8k4) instead of scalar FMAs
 int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
-              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights = nullptr);
+              const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights = nullptr,
+              bool tensor_cores = true);
 // element matrices of a level (the stored form of the on-the-fly operator)
 int element_matrices(int nl, int nr, const double* coords, const double* radii, const double* k, const double* kq0,
                      double* mats, cudaStream_t st);

@@ -254,7 +254,8 @@ struct EpsDivDivOp : Operator {
 // TwoGridGCA (gca.hpp:41-531): coarse.mats = sum P^T A_fine P with A_fine the
 // fine operator's stored matrices or its on-the-fly Neumann element matrices.
 // linear: InterpolationMode::Linear (the fine level's linear-transfer weights) instead of Constant.
-void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear = false);
+void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, bool linear = false,
+                 bool tensor_cores = true);
 
 // B (DivergenceKerngen): velocity level -> pressure level (level - 1).
 struct DivergenceOp : Operator {
@@ -289,5 +290,14 @@ struct StokesOp : Operator {
 
 template <typename T>
 void zero_components(int64_t n, int ncomp, T* const* v, cudaStream_t st);
+
+// XDMF output / checkpoint in the reference's format (xdmf.cpp)
+struct Xdmf;
+Xdmf* xdmf_create(const Shell* sh, int level, const std::string& dir, int geometry_bytes);
+void  xdmf_add(Xdmf* x, const std::string& name, int precision, int ncomp, void* const* comps, int out_bytes);
+void  xdmf_write(Xdmf* x);
+void  xdmf_destroy(Xdmf* x);
+void  xdmf_read(const Shell* sh, int level, const std::string& dir, const std::string& name, int step, int precision,
+                int ncomp, void* const* comps);
 
 }  // namespace tn

@@ -109,7 +109,7 @@ def load(path: str = LIB_PATH):
         "tn_restrict": ([vp, i, i, i, vpp, vpp, vp], i),
         "tn_prolongate_linear_add": ([vp, i, i, i, vpp, vpp, vp], i),
         "tn_restrict_linear": ([vp, i, i, i, vpp, vpp, vp], i),
-        "tn_gca_build_interpolated": ([vp, vp, i, vp], i),
+        "tn_gca_build_interpolated": ([vp, vp, i, i, vp], i),
         "tn_interface_sum": ([vp, i, i, i, vpp, vp], i),
         "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
         "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
@@ -138,6 +138,11 @@ def load(path: str = LIB_PATH):
         "tn_solver_inverse_diagonal": ([vp, i, vpp, vp], i),
         "tn_solver_coarse_stats": ([vp, dp], i),
         "tn_solver_level_matrices": ([vp, i, vp], i),
+        "tn_xdmf_create": ([vp, i, ctypes.c_char_p, i, ctypes.POINTER(vp)], i),
+        "tn_xdmf_add": ([vp, ctypes.c_char_p, i, i, vpp, i], i),
+        "tn_xdmf_write": ([vp, vp], i),
+        "tn_xdmf_destroy": ([vp], None),
+        "tn_xdmf_read": ([vp, i, ctypes.c_char_p, ctypes.c_char_p, i, i, i, vpp], i),
         "tn_vec_invert": ([vp, i, i, i, vpp, vp], i),
         "tn_vec_scale": ([vp, i, i, i, vpp, vpp, vp], i),
         "tn_vec_max_abs": ([vp, i, i, i, vpp, dp, vp], i),
@@ -392,9 +397,9 @@ class EpsDivDiv(Operator):
         return out
 
 
-def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None, interpolation=0):
-    """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build / tn_gca_build_interpolated)."""
-    _check(load().tn_gca_build_interpolated(fine._h, coarse._h, interpolation, _stream(stream)))
+def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None, interpolation=0, tensor_cores=True):
+    """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build_interpolated)."""
+    _check(load().tn_gca_build_interpolated(fine._h, coarse._h, interpolation, int(tensor_cores), _stream(stream)))
 
 
 def random_vector(shell: Shell, level: int, ncomp: int, seed: int, dtype=None, stream=None):
@@ -715,3 +720,36 @@ class MultigridSolver(VelocitySolver):
                                                  bc_surface, ctypes.byref(self.options), _stream(stream),
                                                  ctypes.byref(h)))
         self._h = h
+
+
+class XdmfWriter:
+    """XDMF output / checkpoint of one shell level in the reference's file format (tn_xdmf_*). Fields are added
+    before the first write; every write() stores their current values as a new step."""
+
+    def __init__(self, shell: Shell, level: int, directory: str, geometry_bytes: int = 4):
+        self.shell, self.level = shell, level % shell.num_levels
+        self._keep = []
+        h = ctypes.c_void_p()
+        _check(load().tn_xdmf_create(shell.handle, self.level, directory.encode(), geometry_bytes, ctypes.byref(h)))
+        self._h = h
+
+    def add(self, name: str, field, output_bytes: int = 4):
+        cs = _comps(field)
+        self._keep.append(cs)
+        _check(load().tn_xdmf_add(self._h, name.encode(), _prec(cs[0].dtype), len(cs), _ptrs(cs), output_bytes))
+
+    def write(self, stream=None):
+        _check(load().tn_xdmf_write(self._h, _stream(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tn_xdmf_destroy(self._h)
+            self._h = None
+
+
+def xdmf_read(shell: Shell, level: int, directory: str, name: str, step: int, out):
+    """Restore field `name` of `step` from an XDMF checkpoint directory into `out` (tn_xdmf_read)."""
+    cs = _comps(out)
+    _check(load().tn_xdmf_read(shell.handle, level % shell.num_levels, directory.encode(), name.encode(), step,
+                               _prec(cs[0].dtype), len(cs), _ptrs(cs)))
+    return out

@@ -144,3 +144,21 @@ def test_vcycle_linear_transfers_match_oracle(cuda, gca):
     x = torch.zeros(sh.vec_shape, dtype=torch.float64, device=cuda)
     solver.vcycle(x, _t(b))
     assert rel_err(x.cpu().numpy(), ref) < 1e-9
+
+
+def test_gca_tensor_cores_equal_scalar(cuda):
+    """The FP64 tensor-core triple products of the GCA build equal the scalar ones (1e-13) and the oracle's."""
+    level = 4
+    sh = O.Shell(level)
+    k = smooth_viscosity(sh, 51, 1000.0)
+    g = T.Shell(level, num_levels=2)
+    fine = T.EpsDivDiv(g, 1, k=_t(k), bc_cmb=0, bc_surface=0)
+    nc = sh.coarser().nl
+    out = {}
+    for tc in (True, False):
+        coarse = T.EpsDivDiv(g, 0, k=_t(np.ones((10, nc, nc, nc))), bc_cmb=0, bc_surface=0)
+        T.gca_build(fine, coarse, tensor_cores=tc)
+        out[tc] = coarse.local_matrices()
+    assert rel_err(out[True], out[False]) < 1e-13
+    ref = O.gca_coarsen(O.EpsDivDiv(sh, k=k, bc_cmb=O.NEUMANN, bc_surface=O.NEUMANN))
+    assert rel_err(out[True], ref) < 1e-12

@@ -75,7 +75,8 @@ def _args():
                          "once, an exact solve per V-cycle) or pcg (the reference's 50-iteration CG); the other "
                          "one is timed once beside it")
     ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "coupling",
-                                                             "precondition", "adjoint-L5", "solve-L7", "gca-build"],
+                                                             "precondition", "adjoint-L5", "solve-L7", "gca-build",
+                                                             "gca-modes"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
                          "apply; coupling: the L6 B and B^T applies (FP64); precondition: one application of the "
                          "L6 mixed-precision block preconditioner; gca-build: the Galerkin coarse operators of the "
@@ -381,9 +382,20 @@ def run_coupling(a):
                                    "gradient_frac": bytes_b / tg / 1e9 / peak}}), flush=True)
 
 
+# nodal viscosity of the adaptive-GCA comparisons: the benchmark field with log-amplitude ln(1000), contrast 1e6
+# (GCAElementsCollector's absolute threshold of 10 on the reference-coordinate gradient marks 71 of the 640
+# level-2 cells at level 6; at contrast 1e4 it marks none)
+GCA_MODES_LOG_AMPLITUDE = math.log(1000.0)
+
+
 def run_gca_build(a):
-    """TwoGridGCA down the level-6 hierarchy (Neumann L6 operator -> L5 -> L4 -> L3 -> L2): the batched 18 x 18
-    triple products on the FP64 tensor cores (mma m8n8k4) against the same kernel structure with scalar FMAs."""
+    """TwoGridGCA down the level-6 hierarchy (Neumann L6 operator -> L5 -> L4 -> L3 -> L2).
+
+    Full GCA on the benchmark viscosity: the fast build (L5 from the on-the-fly L6 matrices in the rank form
+    P^T g; L4..L2 from stored matrices with the 18 x 18 triple products on the FP64 tensor cores) against the
+    plain scalar build (one fine wedge at a time, fine matrix then P^T A P), per level and in total, and the
+    level-2 matrices of both. Adaptive GCA on a viscosity of contrast 1e6: the marked coarsest cells, the
+    stored cells and bytes of every coarse level against full GCA, and its build time."""
     import numpy as np
     import torch
 
@@ -393,29 +405,110 @@ def run_gca_build(a):
     shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
     fine = NUM_LEVELS - 1
     eta = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA), device="cuda")
-    ops = {fine: T.EpsDivDiv(shell, fine, k=eta, bc_cmb=0, bc_surface=0)}
-    for l in range(fine - 1, -1, -1):
-        nl, nr = shell.dims(l)
-        ops[l] = T.EpsDivDiv(shell, l, k=torch.ones((10, nl, nl, nr), dtype=torch.float64, device="cuda"),
-                             bc_cmb=0, bc_surface=0)
-    times, mats = {}, {}
-    for tc in (True, False):
+
+    def chain(k, mode):
+        ops = {fine: T.EpsDivDiv(shell, fine, k=k, bc_cmb=0, bc_surface=0)}
+        kl = k
+        for l in range(fine - 1, -1, -1):
+            nl, nr = shell.dims(l)
+            kl = kl[:, ::2, ::2, ::2].contiguous()
+            ops[l] = T.EpsDivDiv(shell, l, k=kl, bc_cmb=0, bc_surface=0)
+        marks = T.gca_mark_elements(shell, fine, fine, k) if mode == "adaptive" else None
+        if marks is not None:
+            for l in range(fine - 1, -1, -1):
+                ops[l].set_selective_matrices(l, marks)
+        return ops, marks
+
+    def build_times(ops, tc):
         per = []
         for l in range(fine - 1, -1, -1):
             T.gca_build(ops[l + 1], ops[l], tensor_cores=tc)  # warm-up (also the input of the next level)
             dt, _ = _timed(torch, lambda: T.gca_build(ops[l + 1], ops[l], tensor_cores=tc))
             per.append({"coarse_level": l + (LEVEL - fine), "ms": dt * 1e3})
-        times["tensor_cores" if tc else "scalar"] = per
+        return per
+
+    times, mats = {}, {}
+    for tc in (True, False):
+        ops, _ = chain(eta, "full")
+        times["fast" if tc else "scalar"] = build_times(ops, tc)
         mats[tc] = ops[0].local_matrices()
+        del ops
     diff = float(np.abs(mats[True] - mats[False]).max() / np.abs(mats[False]).max())
     tot = {k: sum(p["ms"] for p in v) for k, v in times.items()}
-    print(json.dumps({"metric": "L6 GCA hierarchy build time", "value": tot["tensor_cores"], "unit": "ms",
+
+    eta4 = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA, log_amplitude=GCA_MODES_LOG_AMPLITUDE), device="cuda")
+    storage = {}
+    for mode in ("adaptive", "full"):
+        ops, marks = chain(eta4, mode)
+        per = build_times(ops, True)
+        storage[mode] = {"build_ms": sum(p["ms"] for p in per), "per_level": [
+            dict(zip(("stored_cells", "bytes"), ops[l].stored_cells()), level=l + (LEVEL - fine),
+                 cells=10 * (shell.dims(l)[0] - 1) ** 2 * (shell.dims(l)[1] - 1)) for l in range(fine - 1, -1, -1)]}
+        if marks is not None:
+            storage[mode]["marked_coarsest_cells"] = int(marks.sum().item())
+            storage[mode]["coarsest_cells"] = int(marks.numel())
+        del ops
+    for mode in storage:
+        storage[mode]["bytes"] = sum(p["bytes"] for p in storage[mode]["per_level"])
+    print(json.dumps({"metric": "L6 GCA hierarchy build time", "value": tot["fast"], "unit": "ms",
                       "n_gpus": 1, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
                       "config": {"workload": "TwoGridGCA chain of the L6 hierarchy (Neumann L6 operator with the "
                                              "benchmark viscosity, coarse levels 5..2)"},
                       "per_level": times, "scalar_total_ms": tot["scalar"],
-                      "speedup_tensor_cores": tot["scalar"] / tot["tensor_cores"],
-                      "level2_max_rel_diff_tensor_vs_scalar": diff}), flush=True)
+                      "speedup_fast_vs_scalar": tot["scalar"] / tot["fast"],
+                      "level2_max_rel_diff_fast_vs_scalar": diff,
+                      "adaptive_vs_full": {"viscosity": "benchmark field with log-amplitude ln(1000) (contrast 1e6)",
+                                           **storage}}), flush=True)
+
+
+def run_gca_modes(a):
+    """The L6 mixed-precision Stokes solve with full (gca = 1), adaptive (gca = 2) and no GCA (gca = 0) on a
+    nodal viscosity of contrast 1e6: set-up time, iterations and time to 1e-8, the time of one preconditioner
+    application (one FP32 V-cycle), and the bytes of stored coarse-level matrices of each hierarchy."""
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    fine = NUM_LEVELS - 1
+    eta = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA, log_amplitude=GCA_MODES_LOG_AMPLITUDE), device="cuda")
+    temp = S.temperature(shell, fine, seed=SEED_TEMP)
+    f = S.buoyancy_rhs(shell, fine, temp, *BCS)
+    x = _stokes_vectors(torch, shell, fine, "cuda")
+    b = [f[c].contiguous() for c in range(3)] + [torch.zeros_like(x[3])]
+    out = {}
+    for gca in (1, 2, 0):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol = T.StokesSolver(shell, eta=eta, bc_cmb=BCS[0], bc_surface=BCS[1], mixed_precision=1, gca=gca,
+                             coarse_solver=T.COARSE_DENSE, relative_tolerance=1e-8, absolute_tolerance=0.0,
+                             max_iterations=3000, project_pressure_mean=1)
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        for t in x:
+            t.zero_()
+        sol.solve(x, b)  # warm-up
+        dt, _ = _timed(torch, lambda: ([t.zero_() for t in x], sol.solve(x, b)))
+        its, rr, conv = sol.result()
+        # one preconditioner application (Schur step, B^T, one FP32 V-cycle), L2 flushed before each
+        z = [torch.zeros_like(t) for t in b]
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            sol.precondition(b, z)
+        t_prec = _time_device(torch, lambda: sol.precondition(b, z), 10, flush)
+        out[f"gca{gca}"] = {"setup_s": setup, "solve_s": dt, "iterations": its, "relative_residual": rr,
+                            "converged": conv, "precondition_ms": t_prec * 1e3,
+                            "stored_bytes": sum(sol.level_storage(l)[1] for l in range(fine)),
+                            "stored_cells": [sol.level_storage(l)[0] for l in range(fine)]}
+        del sol
+    print(json.dumps({"metric": "L6 mixed-precision Stokes solve time by GCA mode", "value": out["gca2"]["solve_s"],
+                      "unit": "s/solve", "n_gpus": 1, "higher_is_better": False, "dtype": "f32+f64",
+                      "data": "synthetic",
+                      "config": {"workload": "L6 Stokes (no-slip CMB, free-slip surface), buoyancy rhs, viscosity "
+                                             "of contrast 1e6 (benchmark field, log-amplitude ln(1000)), FGMRES(30) "
+                                             "to 1e-8 with the FP32 V-cycle and the dense coarsest solve"},
+                      "modes": out}), flush=True)
 
 
 def run_precondition(a):
@@ -896,6 +989,8 @@ def main():
         run_precondition(a)
     elif a.workload == "gca-build":
         run_gca_build(a)
+    elif a.workload == "gca-modes":
+        run_gca_modes(a)
     elif a.workload == "adjoint-L5":
         run_adjoint_l5(a)
     elif a.workload == "solve-L7":

@@ -9,7 +9,9 @@
  * that contain an input array must be readable device memory (true for any
  * array inside a cudaMalloc / torch allocation).
  * Operations run asynchronously on the caller's CUDA stream (NULL = legacy
- * default stream) unless documented as synchronous.
+ * default stream) unless documented as synchronous. An object lives on the
+ * device that was current when it was created, and that device must be the
+ * current one whenever the object (or anything built on it) is used.
  *
  * Data layout is the reference's diamond-grid layout (src/terra/grid/
  * grid_types.hpp:12-113, Kokkos::LayoutRight): a nodal scalar field is
@@ -155,8 +157,9 @@ int tn_epsdivdiv_vjp(tn_operator* op, const void* const* u_dev, const void* cons
  * the reference. For callers that cannot allocate device memory when they
  * apply the operator. Calls that overlap in time share the scratch and race;
  * the first call on a device does the set-up (looks up the scratch address)
- * and should come before any stream capture. u_dev: 3 velocity components,
- * p_dev: pressure. */
+ * and should come before any stream capture. The scratch used is the current
+ * device's, so the shell's device must be current. u_dev: 3 velocity
+ * components, p_dev: pressure. */
 int tn_divergence_apply_noalloc(tn_shell* shell, int velocity_level, int precision, int bc_cmb, int bc_surface,
                                 const void* const* u_dev, void* p_dev, void* stream);
 
@@ -290,11 +293,37 @@ int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream);
 /* TwoGridGCA with its interpolation_mode argument (gca.hpp:72-78):
  * TN_TRANSFER_CONSTANT (InterpolationMode::Constant, tn_gca_build) or
  * TN_TRANSFER_LINEAR (InterpolationMode::Linear: P from the linear-transfer
- * weights, gca.hpp:231-243, :327-342). tensor_cores = 1 runs the batched 18 x 18
- * triple products P^T A P on the FP64 tensor cores (the default of tn_gca_build
- * and of the solvers), 0 as scalar FMAs. Synchronous. */
+ * weights, gca.hpp:231-243, :327-342). tensor_cores = 1 (the default of
+ * tn_gca_build and of the solvers) is the fast build: over stored fine matrices
+ * the batched 18 x 18 triple products P^T A P run on the FP64 tensor cores; over
+ * on-the-fly fine matrices, which have the form k|J| (g g^T terms) of the wedge
+ * gradients g, the product is formed directly from the gradients P^T g (the same
+ * matrices to rounding). 0: the plain scalar triple product one fine wedge at a
+ * time. Synchronous. */
 int tn_gca_build_interpolated(tn_operator* fine, tn_operator* coarse, int interpolation, int tensor_cores,
                               void* stream);
+/* GCAElementsCollector (src/terra/linalg/solvers/gca/gca_elements_collector.hpp:
+ * 32-105): for each wedge of level `level`, the gradient of the nodal
+ * coefficient k_dev in reference coordinates at the one-point rule's point; where
+ * its norm exceeds 10 the ancestor cell level_range levels coarser is marked.
+ * marks_dev: one byte per cell of level level - level_range (10, n-1, n-1,
+ * nr-1), cleared first, 1 = marked. */
+int tn_gca_mark_elements(tn_shell* shell, int level, int level_range, const double* k_dev, uint8_t* marks_dev,
+                         void* stream);
+/* set_stored_matrix_mode(Selective, level_range, GCAElements) (epsilon_divdiv_
+ * kerngen.hpp:503-528; LocalMatrixStorage, local_matrix_storage.hpp:22-166):
+ * the cells whose ancestor level_range levels coarser is marked in marks_dev
+ * (as from tn_gca_mark_elements) take stored matrices, which a following
+ * tn_gca_build fills; every other cell keeps the on-the-fly operator of the
+ * operator's FP64 nodal coefficient (the slow path's per-cell choice, :1047-
+ * 1060). A selective fine operator coarsens only into a selective coarse
+ * operator with the same marks (TwoGridGCA builds the marked coarse cells, whose
+ * fine children are all stored). Synchronous. */
+int tn_operator_set_selective_matrices(tn_operator* op, int level_range, const uint8_t* marks_dev, void* stream);
+/* cells with stored matrices (all cells in TN_STORED_FULL, the marked ones when
+ * selective, 0 matrix-free) and the device bytes the stored matrices take (no
+ * counterpart in the reference). */
+int tn_operator_stored_cells(tn_operator* op, int64_t* stored_cells, int64_t* bytes);
 /* get_local_matrix for every cell: host array (10, nl-1, nl-1, nr-1, 2, 18, 18),
  * dimension-wise ordering (row = node + 6 * component), without boundary
  * treatment. Synchronous. */
@@ -316,7 +345,10 @@ typedef struct tn_solver_options {
     int      coarse_max_iterations;     /* coarsest-level CG (50) */
     double   coarse_relative_tolerance; /* 1e-6 */
     double   coarse_absolute_tolerance; /* 1e-16 */
-    int      gca;                       /* 1: Galerkin coarse operators on all coarse levels, 0: rediscretised (1) */
+    int      gca;                       /* 1: Galerkin coarse operators on all coarse levels, 0: rediscretised,
+                                           2: adaptive -- Galerkin matrices only on the cells below coarsest cells
+                                           that GCAElementsCollector marks from the fine viscosity, rediscretised
+                                           elsewhere (StokesSolverParameters::gca, parameters.hpp:166-176) (1) */
     int      mixed_precision;           /* 1: FP32 V-cycle inside the FP64 outer iteration (0) */
     uint64_t seed;                      /* power-iteration start vectors (12345) */
     int      normalize_pressure;        /* Stokes: subtract the owned-node pressure mean after the solve, as
@@ -411,8 +443,12 @@ int tn_solver_coarse_stats(tn_solver* solver, double* stats3);
 int tn_stokes_misfit_gradient(tn_solver* solver, const double* const* x_dev, const double* const* u_obs_dev,
                               double* grad_logeta_cell_dev, double* const* lambda_dev, void* stream);
 /* stored matrices of coarse level 0..fine-1 of the hierarchy, layout as
- * tn_operator_copy_local_matrices. */
+ * tn_operator_copy_local_matrices (adaptive GCA: the element matrices of the
+ * rediscretised operator on unmarked cells). */
 int tn_solver_level_matrices(tn_solver* solver, int level, double* mats_host);
+/* stored cells and bytes of level 0..fine of the hierarchy (as
+ * tn_operator_stored_cells). */
+int tn_solver_level_storage(tn_solver* solver, int level, int64_t* stored_cells, int64_t* bytes);
 
 /* ---- XDMF output that doubles as a checkpoint ------------------------------
  * The file format of the reference's XDMFOutput (src/terra/io/xdmf.hpp:13-148,

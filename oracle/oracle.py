@@ -778,6 +778,53 @@ def inject(coarse: Shell, fine_field):
     return np.ascontiguousarray(fine_field[:, ::2, ::2, ::2])
 
 
+def gca_marks(fine: Shell, k, level_range):
+    """GCAElementsCollector (gca_elements_collector.hpp:49-103): per wedge of every fine cell the gradient of the
+    nodal k in reference coordinates at (1/3, 1/3, 0) (grad_shape, integrands.hpp:228-235, summed over the six
+    nodes in order with separate roundings); where its norm exceeds 10 the ancestor cell level_range halvings
+    coarser (map_to_coarse_element) is marked. Returns a bool array over the coarse cells."""
+    k = np.asarray(k, np.float64)
+    nl, nr = fine.nl, fine.nr
+    nlc, nrc = ((nl - 1) >> level_range) + 1, ((nr - 1) >> level_range) + 1
+    marks = np.zeros((10, nlc - 1, nlc - 1, nrc - 1), bool)
+    offs = [[(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (0, 1, 1)],
+            [(1, 1, 0), (0, 1, 0), (1, 0, 0), (1, 1, 1), (0, 1, 1), (1, 0, 1)]]
+    third = 1.0 / 3.0
+    slat = [1.0 - third - third, third, third]
+    gxi, geta = [-1.0, 1.0, 0.0], [-1.0, 0.0, 1.0]
+    hit = np.zeros((10, nl - 1, nl - 1, nr - 1), bool)
+    for w in range(2):
+        g = [np.zeros((10, nl - 1, nl - 1, nr - 1)) for _ in range(3)]
+        for n, (ox, oy, orr) in enumerate(offs[w]):
+            kn = k[:, ox:ox + nl - 1, oy:oy + nl - 1, orr:orr + nr - 1]
+            m, grad = n % 3, (-0.5 if n < 3 else 0.5)
+            g[0] = g[0] + (gxi[m] * 0.5) * kn
+            g[1] = g[1] + (geta[m] * 0.5) * kn
+            g[2] = g[2] + (slat[m] * grad) * kn
+        hit |= np.sqrt(((0.0 + g[0] * g[0]) + g[1] * g[1]) + g[2] * g[2]) > 10.0
+    d, x, y, r = np.nonzero(hit)
+    marks[d, x >> level_range, y >> level_range, r >> level_range] = True
+    return marks
+
+
+def expand_marks(marks, levels):
+    """marks of coarse cells -> marks of their descendants `levels` levels finer."""
+    m = marks
+    for _ in range(levels):
+        m = m.repeat(2, axis=1).repeat(2, axis=2).repeat(2, axis=3)
+    return m
+
+
+def element_matrices(op: "EpsDivDiv"):
+    """get_local_matrix of every cell of an operator without stored matrices: (10, nl-1, nl-1, nr-1, 2, 18, 18)."""
+    sh = op.shell
+    out = np.zeros(sh.cell_shape + (2, 18, 18))
+    for d, x, y, r in np.ndindex(*sh.cell_shape):
+        for w in range(2):
+            out[d, x, y, r, w] = op.local_matrix(d, x, y, r, w)
+    return out
+
+
 class VelocityHierarchy:
     """Multigrid hierarchy as the product builds it (levels[0] coarsest):
     GCA coarse operators (TwoGridGCA top-down, stokes_solver.hpp:375-389) or
@@ -794,9 +841,24 @@ class VelocityHierarchy:
         ops = [None] * num_levels
         ops[-1] = EpsDivDiv(fine, k=k, bc_cmb=bc_cmb, bc_surface=bc_surface)
         self.mats = [None] * num_levels
+        self.marks = None
+        if gca == 2:
+            # adaptive GCA (stokes_solver.hpp:278-287, :360-366): the Galerkin matrices of the full chain on the
+            # cells below marked coarsest cells (their fine children are marked too, so the selective chain
+            # reproduces the full one there), the rediscretised operator's element matrices elsewhere
+            self.marks = gca_marks(fine, k, num_levels - 1)
+            full = VelocityHierarchy(fine, k, bc_cmb, bc_surface, num_levels, gca=1, lambdas=lambdas,
+                                     cheb_order=cheb_order, cheb_iters=cheb_iters, coarse_max_iter=coarse_max_iter,
+                                     coarse_rtol=coarse_rtol, coarse_atol=coarse_atol, transfer=transfer)
         kk = k
         for l in range(num_levels - 2, -1, -1):
-            if gca:
+            if gca == 2:
+                kk = inject(shells[l], kk)
+                ml = expand_marks(self.marks, l)[..., None, None, None]
+                rediscretised = element_matrices(EpsDivDiv(shells[l], k=kk, bc_cmb=bc_cmb, bc_surface=bc_surface))
+                self.mats[l] = np.where(ml, full.mats[l], rediscretised)
+                ops[l] = EpsDivDiv(shells[l], k=kk, bc_cmb=bc_cmb, bc_surface=bc_surface, stored=self.mats[l])
+            elif gca:
                 lin = transfer == "linear"
                 if l == num_levels - 2:
                     src = EpsDivDiv(shells[l + 1], k=k, bc_cmb=NEUMANN, bc_surface=NEUMANN)

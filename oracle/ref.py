@@ -77,6 +77,8 @@ def lib(threads: int = 0):
         L.tnr_epsdivdiv_time.argtypes = [I, D, D, dp, I, I, dp, I, dp]
         L.tnr_rhs_enforce.argtypes = [I, D, D, I, I, dp]
         L.tnr_xdmf_write.argtypes = [I, D, D, ctypes.c_char_p, I, dp, dp, I]
+        L.tnr_gca_marks.argtypes = [I, I, D, D, dp, dp]
+        L.tnr_stokes_level_apply.argtypes = [ctypes.c_void_p, I, I, dp, dp]
         _check(L, L.tnr_init(int(threads) if threads > 0 else (os.cpu_count() or 1)))
         _lib = L
     return _lib
@@ -193,6 +195,15 @@ def gca(fine_lat, coarse_lat, k, linear=False, r_min=0.55, r_max=1.0):
     return out
 
 
+def gca_marks(lat, level_range, k, r_min=0.55, r_max=1.0):
+    """GCAElementsCollector on level lat: bool marks of the cells of level lat - level_range."""
+    nc = _sizes(lat - level_range)
+    out = np.zeros((10, nc - 1, nc - 1, nc - 1))
+    L = lib()
+    _check(L, L.tnr_gca_marks(lat, level_range, r_min, r_max, _dp(_c(k)), _dp(out)))
+    return out > 0.5
+
+
 def prolongate_linear_add(fine_lat, coarse_v, fine_v, r_min=0.55, r_max=1.0):
     """fine += P coarse with ProlongationLinear per component."""
     out = _c(fine_v).copy()
@@ -262,6 +273,15 @@ class StokesRef:
         _check(L, L.tnr_stokes_solve(self._h, rtol, atol, max_it, _dp(b), _dp(x), _dp(hist), len(hist),
                                      ctypes.byref(n), ctypes.byref(t)))
         return x, hist[: n.value].copy(), t.value
+
+    def level_apply(self, level, src, diagonal=False):
+        """A_l src of hierarchy level `level` (0 = coarsest; the fine block at the top), Replace mode with the
+        interface sum; src is (3, 10, n, n, nr)."""
+        src = _c(src)
+        out = np.zeros_like(src)
+        L = lib()
+        _check(L, L.tnr_stokes_level_apply(self._h, level, int(diagonal), _dp(src), _dp(out)))
+        return out
 
     def close(self):
         if self._h:

@@ -74,6 +74,7 @@ void randomize( VectorQ1Vec< double, 3 >& v );
 #include "terra/linalg/solvers/diagonal_solver.hpp"
 #include "terra/linalg/solvers/fgmres.hpp"
 #include "terra/linalg/solvers/gca/gca.hpp"
+#include "terra/linalg/solvers/gca/gca_elements_collector.hpp"
 #include "terra/linalg/solvers/multigrid.hpp"
 #include "terra/linalg/solvers/pcg.hpp"
 #include "terra/linalg/vector_q1isoq2_q1.hpp"
@@ -522,6 +523,31 @@ int tnr_gca( int fine_lat, int coarse_lat, double r_min, double r_max, const dou
     } );
 }
 
+/// GCAElementsCollector (gca_elements_collector.hpp:49-103) on level lat with nodal coefficient k: out (one
+/// value per cell of level lat - level_range, (10, n-1, n-1, nr-1)) receives the GCAElements entries of those
+/// cells (1 where marked, else 0).
+int tnr_gca_marks( int lat, int level_range, double r_min, double r_max, const double* k, double* out )
+{
+    return guarded( [&] {
+        if ( level_range < 0 || lat - level_range < 0 )
+            throw std::runtime_error( "bad level range" );
+        Level& F = level( lat, lat, r_min, r_max );
+        Level& C = level( lat - level_range, lat - level_range, r_min, r_max );
+        VectorQ1Scalar< double > elements( "GCAElements", *C.domain, C.owned );
+        linalg::assign( elements, 0.0 );
+        auto kf = scalar_field( F, k, "k" );
+        linalg::solvers::GCAElementsCollector< double >( *F.domain, kf, level_range, elements.grid_data() );
+        Kokkos::fence();
+        const auto& e = elements.grid_data();
+        long        o = 0;
+        for ( int sd = 0; sd < 10; ++sd )
+            for ( int x = 0; x < C.nl - 1; ++x )
+                for ( int y = 0; y < C.nl - 1; ++y )
+                    for ( int r = 0; r < C.nr - 1; ++r )
+                        out[o++] = e( sd, x, y, r );
+    } );
+}
+
 /// The Stokes solve of the application (stokes_solver.hpp:169-610 set-up, :644-691 solve without the pressure
 /// normalisation): FGMRES(restart) with the block-triangular preconditioner; velocity block = Multigrid V-cycles
 /// with Chebyshev(order, iterations, power_iterations) smoothing on levels lat-num_levels+1 .. lat, GCA coarse
@@ -595,15 +621,18 @@ int tnr_stokes_create( int lat, int num_levels, double r_min, double r_max, int 
 
         Level&                   L0 = *S->lv[0];
         VectorQ1Scalar< double > elements( "GCAElements", *L0.domain, L0.owned );
-        linalg::assign( elements, gca ? 1.0 : 0.0 );
+        linalg::assign( elements, gca == 1 ? 1.0 : 0.0 );
+        if ( gca == 2 ) // adaptive GCA (stokes_solver.hpp:278-287)
+            linalg::solvers::GCAElementsCollector< double >( *F.domain, kf, num_levels - 1, elements.grid_data() );
         for ( int l = 0; l < num_levels - 1; ++l )
         {
             Level& L = *S->lv[l];
             S->A_c.emplace_back( *L.domain, L.coords, L.radii, L.boundary,
                                  scalar_field( L, k_levels ? k_levels[l] : nullptr, "k_c" ), bcs, false );
             if ( gca )
-                S->A_c.back().set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, l,
-                                                      elements.grid_data() );
+                S->A_c.back().set_stored_matrix_mode( gca == 2 ? linalg::OperatorStoredMatrixMode::Selective :
+                                                                 linalg::OperatorStoredMatrixMode::Full,
+                                                      l, elements.grid_data() );
             S->Pv.emplace_back( linalg::OperatorApplyMode::Add );
             S->Rv.emplace_back( *L.domain );
         }
@@ -718,6 +747,28 @@ int tnr_stokes_solve( void* h, double rtol, double atol, int max_it, const doubl
 void tnr_stokes_destroy( void* h )
 {
     delete static_cast< StokesRef* >( h );
+}
+
+/// dst = A_l src with operator l (0 = coarsest) of the velocity hierarchy of a StokesRef (A_c[l], the fine
+/// block for l = num_levels - 1), Replace + CommunicateAdditively, in diagonal mode when diagonal != 0.
+/// src, dst: 3 components of the level's nodes.
+int tnr_stokes_level_apply( void* h, int l, int diagonal, const double* src, double* dst )
+{
+    return guarded( [&] {
+        auto*     S = static_cast< StokesRef* >( h );
+        const int n = static_cast< int >( S->lv.size() );
+        if ( l < 0 || l >= n )
+            throw std::runtime_error( "level out of range" );
+        Level&                L = *S->lv[l];
+        auto&                 A = ( l == n - 1 ) ? S->K->block_11() : S->A_c[l];
+        VectorQ1Vec< double > u( "u", *L.domain, L.owned ), v( "v", *L.domain, L.owned );
+        load( u.grid_data(), src );
+        A.set_diagonal( diagonal != 0 );
+        linalg::apply( A, u, v );
+        A.set_diagonal( false );
+        Kokkos::fence();
+        store( v.grid_data(), dst );
+    } );
 }
 
 /// Wall time of `reps` consecutive EpsilonDivDivKerngen<double> applies (Replace + CommunicateAdditively, fast

@@ -121,7 +121,7 @@ tn::MgOptions mg_options(const tn_solver_options& o)
     m.transfer        = o.transfer == TN_TRANSFER_LINEAR ? 1 : 0;
     need(o.transfer == TN_TRANSFER_CONSTANT || o.transfer == TN_TRANSFER_LINEAR, "unknown transfer");
     need(o.coarse_solver == TN_COARSE_PCG || o.coarse_solver == TN_COARSE_DENSE, "unknown coarse solver");
-    need(o.gca == 0 || o.gca == 1, "gca must be 0 or 1");
+    need(o.gca == 0 || o.gca == 1 || o.gca == 2, "gca must be 0, 1 or 2");
     need(o.smoother == TN_SMOOTHER_CHEBYSHEV || o.smoother == TN_SMOOTHER_JACOBI, "unknown smoother");
     need(o.jacobi_omega > 0.0, "jacobi_omega must be positive");
     return m;
@@ -130,10 +130,16 @@ tn::MgOptions mg_options(const tn_solver_options& o)
 // stored packed matrices -> (cells, 2, 18, 18) full symmetric host array
 void unpack_matrices(const tn::EpsDivDivOp& op, double* mats_host)
 {
-    need(op.stored && op.mats.get(), "the operator has no stored matrices");
+    need((op.stored && op.mats.get()) || (op.selective && op.sel_built), "the operator has no stored matrices");
     const int64_t       nc = op.lvl().cells();
     std::vector<double> packed(static_cast<size_t>(tn::gca_values_per_cell()) * nc);
-    tn::cuda_check(cudaMemcpy(packed.data(), op.mats.get(), packed.size() * sizeof(double), cudaMemcpyDeviceToHost),
+    tn::DevBuf          eff;  // selective storage: stored matrices on marked cells, element matrices elsewhere
+    if (op.selective) {
+        op.effective_matrices(eff, nullptr);
+        tn::cuda_check(cudaStreamSynchronize(nullptr), "assemble matrices");
+    }
+    tn::cuda_check(cudaMemcpy(packed.data(), op.selective ? eff.get() : op.mats.get(), packed.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost),
                    "copy matrices");
     for (int64_t c = 0; c < nc; ++c)
         for (int w = 0; w < 2; ++w) {
@@ -832,6 +838,40 @@ int tn_operator_set_stored_matrix_mode(tn_operator* op, int mode, void* stream)
     });
 }
 
+int tn_gca_mark_elements(tn_shell* shell, int level, int level_range, const double* k_dev, uint8_t* marks_dev,
+                         void* stream)
+{
+    return guarded([&] {
+        need(shell && k_dev && marks_dev, "NULL argument");
+        const auto& L = shell->impl->level(level);
+        need(level_range >= 0 && level - level_range >= 0, "level_range must lead to a level of the shell");
+        const auto& Lc = shell->impl->level(level - level_range);
+        tn::cuda_check(cudaMemsetAsync(marks_dev, 0, static_cast<size_t>(Lc.cells()), as_stream(stream)),
+                       "clear marks");
+        if (tn::gca_mark_elements(L.nl(), L.nr(), k_dev, level_range, marks_dev, as_stream(stream)) != 0)
+            throw tn::Error(tn::kErrCuda, "marking launch failed");
+    });
+}
+
+int tn_operator_set_selective_matrices(tn_operator* op, int level_range, const uint8_t* marks_dev, void* stream)
+{
+    return guarded([&] {
+        need(op && marks_dev, "NULL argument");
+        as_edd(op)->set_selective(marks_dev, level_range, as_stream(stream));
+    });
+}
+
+int tn_operator_stored_cells(tn_operator* op, int64_t* stored_cells, int64_t* bytes)
+{
+    return guarded([&] {
+        need(op && stored_cells && bytes, "NULL argument");
+        const auto* e = as_edd(op);
+        *stored_cells = e->selective ? e->sel_count : (e->stored ? e->lvl().cells() : 0);
+        *bytes = static_cast<int64_t>(e->mats.size() + e->sel_delta.size() + e->baked64.size() + e->baked32.size() +
+                                      e->sel_cells.size() + e->sel_slot.size());
+    });
+}
+
 int tn_gca_build(tn_operator* fine, tn_operator* coarse, void* stream)
 {
     return tn_gca_build_interpolated(fine, coarse, TN_TRANSFER_CONSTANT, 1, stream);
@@ -1138,6 +1178,18 @@ int tn_solver_level_matrices(tn_solver* s, int level, double* mats_host)
         need(s && mats_host, "NULL argument");
         need(level >= 0 && level < s->mg().fine_level(), "level must be a coarse level");
         unpack_matrices(s->mg().op64(level), mats_host);
+    });
+}
+
+int tn_solver_level_storage(tn_solver* s, int level, int64_t* stored_cells, int64_t* bytes)
+{
+    return guarded([&] {
+        need(s && stored_cells && bytes, "NULL argument");
+        need(level >= 0 && level <= s->mg().fine_level(), "level out of range");
+        const auto& e = s->mg().op64(level);
+        *stored_cells = e.selective ? e.sel_count : (e.stored ? e.lvl().cells() : 0);
+        *bytes = static_cast<int64_t>(e.mats.size() + e.sel_delta.size() + e.baked64.size() + e.baked32.size() +
+                                      e.sel_cells.size() + e.sel_slot.size());
     });
 }
 

@@ -141,7 +141,9 @@ int dense_invert_spd(int64_t n, double* A, double* colk, cudaStream_t st)
 int dense_coarse_prepare(int unknowns)
 {
     if (unknowns > kDenseCoarseMaxUnknowns) return -2;
-    const size_t smem = sizeof(double) * static_cast<size_t>(unknowns);
+    // The limit is raised to the largest supported system, not to this one:
+    // a smaller solver prepared later must not lower it under a larger one.
+    const size_t smem = sizeof(double) * static_cast<size_t>(kDenseCoarseMaxUnknowns);
     return cudaFuncSetAttribute(dense_gemv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)) == cudaSuccess
                ? 0

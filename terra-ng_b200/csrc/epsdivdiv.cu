@@ -37,6 +37,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <type_traits>
 
 namespace tn {
@@ -606,16 +607,19 @@ int launch_cfg(EddArgs<T> a, int nfields, cudaStream_t st)
     if (L.total > kSmemLimit) return -5;
     auto k = epsdivdiv_kernel<T, CPL, DIAG>;
     // the dynamic shared-memory limit is a per-device attribute of the kernel:
-    // raise it once per device (and only upwards)
-    static std::atomic<size_t> configured[kMaxDevices];
-    int                        dev = 0;
+    // raise it once per device, only upwards; the check, the attribute call
+    // and the record happen under one lock so racing threads cannot lower it
+    static std::mutex mu;
+    static size_t     configured[kMaxDevices];
+    int               dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
-    if (L.total > configured[dev].load(std::memory_order_relaxed)) {
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total)) !=
-            cudaSuccess)
-            return -1;
-        size_t prev = configured[dev].load(std::memory_order_relaxed);
-        while (prev < L.total && !configured[dev].compare_exchange_weak(prev, L.total)) {
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (L.total > configured[dev]) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total)) !=
+                cudaSuccess)
+                return -1;
+            configured[dev] = L.total;
         }
     }
     const int nl = a.nl;

@@ -139,13 +139,18 @@ void iface(const DeviceLevel& L, int ncomp, T* const* v, cudaStream_t st)
 }
 }  // namespace
 
-int64_t EpsDivDivOp::mats_values() const { return static_cast<int64_t>(gca_values_per_cell()) * lvl().cells(); }
+int64_t EpsDivDivOp::mats_values() const
+{
+    return static_cast<int64_t>(gca_values_per_cell()) * (selective ? sel_count : lvl().cells());
+}
 
 void EpsDivDivOp::set_stored_matrices_from_coefficient(cudaStream_t st)
 {
     const DeviceLevel& L = lvl();
     if (precision != 0) throw Error(kErrUnsupported, "stored matrices are assembled from an FP64 coefficient");
     if (k.get() == nullptr) throw Error(kErrState, "operator has no coefficient to assemble matrices from");
+    selective = false;
+    sel_built = false;
     mats.alloc(static_cast<size_t>(mats_values()) * sizeof(double));
     if (element_matrices(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), q0 ? nullptr : k.as<double>(),
                          q0 ? k.as<double>() : nullptr, mats.as<double>(), st) != 0)
@@ -155,17 +160,138 @@ void EpsDivDivOp::set_stored_matrices_from_coefficient(cudaStream_t st)
     baked32_valid = false;
 }
 
-void EpsDivDivOp::ensure_baked(bool need32, cudaStream_t st)
+void EpsDivDivOp::set_selective(const uint8_t* marks_dev, int level_range, cudaStream_t st)
 {
     const DeviceLevel& L = lvl();
-    if (!stored || mats.get() == nullptr) throw Error(kErrState, "stored matrix mode without matrices");
+    if (precision != 0 || k.get() == nullptr)
+        throw Error(kErrUnsupported, "selective storage needs the FP64 coefficient of the on-the-fly operator");
+    const int nl = L.nl(), nr = L.nr();
+    if (level_range < 0 || ((nl - 1) >> level_range) < 1 || ((nr - 1) >> level_range) < 1 ||
+        (((nl - 1) >> level_range) << level_range) != nl - 1 || (((nr - 1) >> level_range) << level_range) != nr - 1)
+        throw Error(kErrArg, "level_range does not lead to a coarser level of this shell");
+    const int nlc = ((nl - 1) >> level_range) + 1, nrc = ((nr - 1) >> level_range) + 1;
+    std::vector<uint8_t> marks(static_cast<size_t>(10) * (nlc - 1) * (nlc - 1) * (nrc - 1));
+    cuda_check(cudaMemcpyAsync(marks.data(), marks_dev, marks.size(), cudaMemcpyDeviceToHost, st), "copy marks");
+    cuda_check(cudaStreamSynchronize(st), "copy marks");
+    const int64_t        nc = L.cells();
+    std::vector<int32_t> cells, slot(static_cast<size_t>(nc), -1);
+    int64_t              c = 0;
+    for (int d = 0; d < 10; ++d)
+        for (int x = 0; x < nl - 1; ++x)
+            for (int y = 0; y < nl - 1; ++y)
+                for (int r = 0; r < nr - 1; ++r, ++c) {
+                    const int64_t a = ((static_cast<int64_t>(d) * (nlc - 1) + (x >> level_range)) * (nlc - 1) +
+                                       (y >> level_range)) *
+                                          (nrc - 1) +
+                                      (r >> level_range);
+                    if (marks[static_cast<size_t>(a)]) {
+                        slot[static_cast<size_t>(c)] = static_cast<int32_t>(cells.size());
+                        cells.push_back(static_cast<int32_t>(c));
+                    }
+                }
+    sel_cells       = upload(cells);
+    sel_slot        = upload(slot);
+    sel_count       = static_cast<int>(cells.size());
+    sel_level_range = level_range;
+    selective       = true;
+    sel_built       = false;
+    stored          = false;
+    mats.release();
+    sel_delta.release();
+    baked64.release();
+    baked32.release();
+    baked_bc[0]   = -1;
+    baked32_valid = false;
+}
+
+void EpsDivDivOp::finish_selective(cudaStream_t st)
+{
+    const DeviceLevel& L = lvl();
+    if (!selective) throw Error(kErrState, "the operator has no selective storage");
+    sel_delta.ensure(static_cast<size_t>(mats_values()) * sizeof(double));
+    if (element_matrices(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), q0 ? nullptr : k.as<double>(),
+                         q0 ? k.as<double>() : nullptr, sel_delta.as<double>(), st, sel_cells.as<int>(), sel_count,
+                         mats.as<double>()) != 0)
+        throw Error(kErrCuda, "correction matrix launch failed");
+    sel_built     = true;
+    baked_bc[0]   = -1;
+    baked32_valid = false;
+}
+
+void EpsDivDivOp::effective_matrices(DevBuf& out, cudaStream_t st) const
+{
+    const DeviceLevel& L  = lvl();
+    const int64_t      nc = L.cells();
+    out.alloc(static_cast<size_t>(gca_values_per_cell()) * nc * sizeof(double));
+    if (stored) {
+        cuda_check(cudaMemcpyAsync(out.get(), mats.get(), out.size(), cudaMemcpyDeviceToDevice, st), "copy");
+        return;
+    }
+    if (k.get() == nullptr || precision != 0) throw Error(kErrState, "no FP64 coefficient to assemble matrices from");
+    if (element_matrices(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), q0 ? nullptr : k.as<double>(),
+                         q0 ? k.as<double>() : nullptr, out.as<double>(), st) != 0)
+        throw Error(kErrCuda, "element matrix assembly launch failed");
+    if (selective && sel_built &&
+        gca_scatter_slots(sel_count, sel_cells.as<int>(), mats.as<double>(), static_cast<int>(nc), out.as<double>(),
+                          st) != 0)
+        throw Error(kErrCuda, "scatter launch failed");
+}
+
+void EpsDivDivOp::materialize_full(cudaStream_t st)
+{
+    if (!selective) return;
+    DevBuf full;
+    effective_matrices(full, st);
+    cuda_check(cudaStreamSynchronize(st), "materialize");
+    mats      = std::move(full);
+    selective = false;
+    sel_built = false;
+    sel_count = 0;
+    sel_cells.release();
+    sel_slot.release();
+    sel_delta.release();
+    baked64.release();
+    baked32.release();
+    stored        = true;
+    baked_bc[0]   = -1;
+    baked32_valid = false;
+}
+
+void EpsDivDivOp::prepare_fp32(cudaStream_t st)
+{
+    if (precision != 0) return;
+    if (selective && k32.get() == nullptr) {
+        const int64_t n = static_cast<int64_t>(k.size() / sizeof(double));
+        DevBuf        b(sizeof(float) * static_cast<size_t>(n));
+        if (convert_f64_to_f32(n, k.as<double>(), b.as<float>(), st) != 0)
+            throw Error(kErrCuda, "conversion launch failed");
+        k32 = std::move(b);
+    }
+    if (penalty_active() && pen_modes32.get() == nullptr) {
+        prepare_penalty(st);
+        const int64_t n = 9 * lvl().nodes();
+        DevBuf        b(sizeof(float) * static_cast<size_t>(n));
+        if (convert_f64_to_f32(n, pen_modes.as<double>(), b.as<float>(), st) != 0)
+            throw Error(kErrCuda, "conversion launch failed");
+        pen_modes32 = std::move(b);
+    }
+    cuda_check(cudaStreamSynchronize(st), "prepare fp32");
+}
+
+void EpsDivDivOp::ensure_baked(bool need32, cudaStream_t st)
+{
+    const DeviceLevel& L   = lvl();
+    const DevBuf&      src = selective ? sel_delta : mats;
+    if (selective ? !sel_built : (!stored || mats.get() == nullptr))
+        throw Error(kErrState, "stored matrix mode without matrices");
     const size_t nv = static_cast<size_t>(mats_values());
+    if (nv == 0) return;
     if (baked_bc[0] != bc_cmb || baked_bc[1] != bc_surf || baked64.get() == nullptr) {
         if (baked64.get() == nullptr) baked64.alloc(nv * sizeof(double));
-        cuda_check(cudaMemcpyAsync(baked64.get(), mats.get(), nv * sizeof(double), cudaMemcpyDeviceToDevice, st),
+        cuda_check(cudaMemcpyAsync(baked64.get(), src.get(), nv * sizeof(double), cudaMemcpyDeviceToDevice, st),
                    "copy matrices");
         if (gca_bake_boundary(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), bc_cmb, bc_surf,
-                              baked64.as<double>(), st) != 0)
+                              baked64.as<double>(), st, selective ? sel_cells.as<int>() : nullptr, sel_count) != 0)
             throw Error(kErrCuda, "boundary bake launch failed");
         baked_bc[0]   = bc_cmb;
         baked_bc[1]   = bc_surf;
@@ -183,16 +309,39 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, 
 {
     if (fine.shell != coarse.shell || coarse.level != fine.level - 1)
         throw Error(kErrArg, "GCA needs operators on consecutive levels of one shell");
-    const DeviceLevel& Lf = fine.lvl();
-    if (!fine.stored && (fine.precision != 0 || fine.k.get() == nullptr))
+    const DeviceLevel& Lf       = fine.lvl();
+    const bool         fine_sel = fine.selective && fine.sel_built;
+    if (!fine.stored && !fine_sel && (fine.precision != 0 || fine.k.get() == nullptr))
         throw Error(kErrUnsupported, "GCA needs an FP64 fine coefficient or stored fine matrices");
-    coarse.mats.alloc(static_cast<size_t>(coarse.mats_values()) * sizeof(double));
-    const double* kf   = (!fine.stored && !fine.q0) ? fine.k.as<double>() : nullptr;
-    const double* kq0f = (!fine.stored && fine.q0) ? fine.k.as<double>() : nullptr;
-    const double* linw = linear ? Lf.linear_weights<double>(st) : nullptr;
+    GcaSlots sl;
+    if (fine_sel) {
+        // TwoGridGCA reads get_local_matrix of the fine children, which a selective store only has for the
+        // children of marked cells (gca.hpp:157-163, epsilon_divdiv_kerngen.hpp:546-562)
+        if (!coarse.selective || coarse.sel_level_range != fine.sel_level_range - 1)
+            throw Error(kErrUnsupported,
+                        "a selectively stored fine operator can only be coarsened into a selective operator "
+                        "with the same marks");
+        sl.fine_slot   = fine.sel_slot.as<int>();
+        sl.fine_stride = fine.sel_count;
+    }
+    if (coarse.selective) {
+        sl.cells  = coarse.sel_cells.as<int>();
+        sl.nslots = coarse.sel_count;
+    }
+    sl.err = coarse.shell->err_word();
+    coarse.mats.ensure(static_cast<size_t>(coarse.mats_values()) * sizeof(double));
+    const bool    on_the_fly = !fine.stored && !fine_sel;
+    const double* kf         = (on_the_fly && !fine.q0) ? fine.k.as<double>() : nullptr;
+    const double* kq0f       = (on_the_fly && fine.q0) ? fine.k.as<double>() : nullptr;
+    const double* linw       = linear ? Lf.linear_weights<double>(st) : nullptr;
     if (gca_build(Lf.nl(), Lf.nr(), Lf.coords<double>(), Lf.radii<double>(), kf, kq0f,
-                  fine.stored ? fine.mats.as<double>() : nullptr, coarse.mats.as<double>(), st, linw, tensor_cores) != 0)
+                  on_the_fly ? nullptr : fine.mats.as<double>(), coarse.mats.as<double>(), st, linw, tensor_cores,
+                  sl) != 0)
         throw Error(kErrCuda, "GCA build launch failed");
+    if (coarse.selective) {
+        coarse.finish_selective(st);
+        return;
+    }
     coarse.stored        = true;
     coarse.baked_bc[0]   = -1;
     coarse.baked32_valid = false;
@@ -262,9 +411,13 @@ void EpsDivDivOp::add_penalty(const T* const* src, T* const* dst, cudaStream_t s
 {
     if (!penalty_active() || diagonal) return;
     prepare_penalty(st);
-    const DeviceLevel& L = lvl();
-    double*            ps = pen_scratch.as<double>();
-    if (penalty_apply<T>(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), src, dst, pen_modes.as<T>(), kPenaltyEpsilon,
+    const DeviceLevel& L      = lvl();
+    double*            ps     = pen_scratch.as<double>();
+    const bool         fp32_of_fp64 = std::is_same<T, float>::value && precision == 0;
+    if (fp32_of_fp64 && pen_modes32.get() == nullptr)
+        throw Error(kErrState, "FP32 apply of an FP64 operator: prepare_fp32 was not called");
+    const T* modes = fp32_of_fp64 ? pen_modes32.as<T>() : pen_modes.as<T>();
+    if (penalty_apply<T>(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), src, dst, modes, kPenaltyEpsilon,
                          ps + 4, ps, st) != 0)
         throw Error(kErrCuda, "penalty launch failed");
 }
@@ -322,15 +475,20 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
         if (comm_mode == 1) iface<T>(L, 3, dst, st);
         return;
     }
+    // matrix-free over every cell; a selective store adds its correction over the stored cells below
+    const bool fp32_of_fp64 = std::is_same<T, float>::value && precision == 0;
+    if (fp32_of_fp64 && (!selective || k32.get() == nullptr))
+        throw Error(kErrState, "FP32 apply of an FP64 matrix-free operator needs prepare_fp32 (selective only)");
+    const T*     kk = fp32_of_fp64 ? k32.as<T>() : k.as<T>();
     EddLaunch<T> p;
     p.nl     = L.nl();
     p.nr     = L.nr();
     p.coords = L.coords<T>();
     p.radii  = L.radii<T>();
     if (q0)
-        p.kq0 = k.as<T>();
+        p.kq0 = kk;
     else
-        p.k = k.as<T>();
+        p.k = kk;
     for (int c = 0; c < 3; ++c) {
         p.src[c] = src[c];
         p.dst[c] = dst[c];
@@ -344,6 +502,22 @@ void EpsDivDivOp::apply_t(const T* const* src, T* const* dst, cudaStream_t st)
     p.err      = shell->err_word();
     const int rc = epsdivdiv_apply<T>(p, st);
     if (rc != 0) throw Error(kErrCuda, "epsdivdiv launch failed (" + std::to_string(rc) + ")");
+    if (selective && sel_built && sel_count > 0) {
+        if (diagonal) {
+            if (!std::is_same<T, double>::value)
+                throw Error(kErrUnsupported, "diagonal mode of a stored operator is FP64 only");
+            if (gca_diag_add(L.nl(), L.nr(), L.coords<double>(), L.radii<double>(), bc_cmb, bc_surf,
+                             sel_delta.as<double>(), reinterpret_cast<const double* const*>(src),
+                             reinterpret_cast<double* const*>(dst), st, sel_cells.as<int>(), sel_count) != 0)
+                throw Error(kErrCuda, "stored diagonal launch failed");
+        } else {
+            ensure_baked(std::is_same<T, float>::value, st);
+            const T* m = std::is_same<T, float>::value ? static_cast<const T*>(baked32.get())
+                                                       : static_cast<const T*>(baked64.get());
+            if (gca_apply_add<T>(L.nl(), L.nr(), m, src, dst, st, sel_cells.as<int>(), sel_count) != 0)
+                throw Error(kErrCuda, "stored apply launch failed");
+        }
+    }
     add_penalty<T>(src, dst, st);
     if (comm_mode == 1) iface<T>(L, 3, dst, st);
 }

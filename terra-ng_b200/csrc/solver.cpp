@@ -171,10 +171,24 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
         op->chunk_x = fine.chunk_x;
         ops64_[fine_] = std::move(op);
     }
-    // coarse levels: Galerkin (TwoGridGCA top-down, stokes_solver.hpp:375-389) or rediscretised
+    // adaptive GCA (gca = 2): GCAElementsCollector on the fine coefficient marks coarsest cells
+    // (stokes_solver.hpp:278-287)
+    DevBuf marks;
+    if (o.gca == 2) {
+        if (fine.q0) throw Error(kErrUnsupported, "adaptive GCA marks cells from a nodal coefficient");
+        const DeviceLevel& L0 = sh->level(0);
+        marks.alloc(static_cast<size_t>(L0.cells()));
+        cuda_check(cudaMemsetAsync(marks.get(), 0, marks.size(), st), "clear marks");
+        const DeviceLevel& Lf = sh->level(fine_);
+        chk(gca_mark_elements(Lf.nl(), Lf.nr(), ops64_[fine_]->k.as<double>(), fine_, marks.as<uint8_t>(), st),
+            "mark GCA elements");
+    }
+    // coarse levels: Galerkin (TwoGridGCA top-down, stokes_solver.hpp:375-389) on every cell (gca = 1), on the
+    // marked cells only with the rediscretised operator elsewhere (gca = 2, OperatorStoredMatrixMode::Selective,
+    // :360-366), or rediscretised (gca = 0)
     for (int l = fine_ - 1; l >= 0; --l) {
         auto op = make_op(l);
-        if (o.gca) {
+        if (o.gca == 1) {
             gca_coarsen(*ops64_[l + 1], *op, st, o.transfer == 1);
         } else {
             const DeviceLevel& Lc = sh->level(l);
@@ -186,10 +200,15 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
                 op->k.alloc(sizeof(double) * Lc.nodes());
                 chk(coefficient_inject(Lc.nl(), Lc.nr(), kf.as<double>(), op->k.as<double>(), false, st), "inject");
             }
+            if (o.gca == 2) {
+                op->set_selective(marks.as<uint8_t>(), l, st);
+                gca_coarsen(*ops64_[l + 1], *op, st, o.transfer == 1);
+            }
         }
         ops64_[l] = std::move(op);
     }
     // the coarsest CG runs over stored matrices
+    ops64_[0]->materialize_full(st);
     if (!ops64_[0]->stored) ops64_[0]->set_stored_matrices_from_coefficient(st);
     ops64_[0]->ensure_baked(false, st);
     {
@@ -214,8 +233,9 @@ VelocityMultigrid::VelocityMultigrid(const Shell* sh, const EpsDivDivOp& fine, c
     // FP32 operators where the apply is matrix-free
     if (o.fp32) {
         for (int l = 1; l <= fine_; ++l) {
-            if (ops64_[l]->stored) {
-                ops64_[l]->ensure_baked(true, st);
+            if (ops64_[l]->stored || ops64_[l]->selective) {
+                ops64_[l]->prepare_fp32(st);
+                if (ops64_[l]->stored || ops64_[l]->sel_count > 0) ops64_[l]->ensure_baked(true, st);
                 continue;
             }
             auto op       = make_op(l);

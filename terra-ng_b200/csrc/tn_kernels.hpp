@@ -157,25 +157,48 @@ int convert_f32_to_f64(int64_t n, const float* in, double* out, cudaStream_t str
 // are packed symmetric, 171 values per wedge, value-major: [w * 171 + p][cell].
 // ----------------------------------------------------------------------------
 int gca_values_per_cell();
+// Selective storage (OperatorStoredMatrixMode::Selective, local_matrix_storage.hpp:22-166): matrices of the
+// listed cells only, slot s of a [342][nslots] array holding cell cells[s]. For a build, cells / nslots
+// name the coarse cells to build and fine_slot (fine cell -> slot, -1 none) / fine_stride the layout of the
+// stored fine matrices; nullptr means every cell with slot = cell. A fine cell without a slot is reported
+// to err (kDevBadLaunch).
+struct GcaSlots {
+    const int* cells       = nullptr;
+    int        nslots      = 0;
+    const int* fine_slot   = nullptr;
+    int        fine_stride = 0;
+    int*       err         = nullptr;
+};
 // coarse = sum P^T A_f P (fine level nlf, nrf); A_f from the nodal / cell
 // coefficient (on-the-fly element matrices) or from stored fine matrices.
-// linear_weights: the fine level's linear-transfer weights for InterpolationMode::Linear, or nullptr (Constant);
-// tensor_cores: the triple products as FP64 tensor-core tiles (mma m8n8k4) instead of scalar FMAs
+// linear_weights: the fine level's linear-transfer weights for InterpolationMode::Linear, or nullptr (Constant).
+// tensor_cores: the fast build -- over on-the-fly fine matrices the rank form of the triple product, over
+// stored ones the triple products as FP64 tensor-core tiles (mma m8n8k4); false: the plain scalar triple
+// product one fine wedge at a time.
 int gca_build(int nlf, int nrf, const double* coords_f, const double* radii_f, const double* k_f, const double* kq0_f,
               const double* fine_mats, double* coarse_mats, cudaStream_t st, const double* linear_weights = nullptr,
-              bool tensor_cores = true);
-// element matrices of a level (the stored form of the on-the-fly operator)
+              bool tensor_cores = true, const GcaSlots& slots = GcaSlots{});
+// element matrices of a level (the stored form of the on-the-fly operator), of every cell or of the listed
+// ones; with base given, mats = base - element matrices
 int element_matrices(int nl, int nr, const double* coords, const double* radii, const double* k, const double* kq0,
-                     double* mats, cudaStream_t st);
+                     double* mats, cudaStream_t st, const int* cells = nullptr, int nslots = 0,
+                     const double* base = nullptr);
+// full[p][cells[s]] = compact[p][s]
+int gca_scatter_slots(int nslots, const int* cells, const double* compact, int ncells, double* full, cudaStream_t st);
+// GCAElementsCollector: marks[coarsest cell] = 1 for the coarsest ancestors (level_range halvings) of cells
+// whose wedges have a reference-coordinate coefficient gradient above 10 (marks is not cleared)
+int gca_mark_elements(int nl, int nr, const double* k, int level_range, uint8_t* marks, cudaStream_t st);
 // bake Dirichlet masks / free-slip rotations of the boundary cells into mats
 int gca_bake_boundary(int nl, int nr, const double* coords, const double* radii, int bc_cmb, int bc_surf, double* mats,
-                      cudaStream_t st);
+                      cudaStream_t st, const int* cells = nullptr, int nslots = 0);
 // dst += A src with baked matrices
 template <typename T>
-int gca_apply_add(int nl, int nr, const T* mats, const T* const* src, T* const* dst, cudaStream_t st);
+int gca_apply_add(int nl, int nr, const T* mats, const T* const* src, T* const* dst, cudaStream_t st,
+                  const int* cells = nullptr, int nslots = 0);
 // dst += diag-mode(A) src with unbaked matrices
 int gca_diag_add(int nl, int nr, const double* coords, const double* radii, int bc_cmb, int bc_surf,
-                 const double* mats, const double* const* src, double* const* dst, cudaStream_t st);
+                 const double* mats, const double* const* src, double* const* dst, cudaStream_t st,
+                 const int* cells = nullptr, int nslots = 0);
 int gca_to_f32(int64_t n, const double* in, float* out, cudaStream_t st);
 
 // ----------------------------------------------------------------------------

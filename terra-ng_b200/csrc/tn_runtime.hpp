@@ -74,6 +74,11 @@ class DevBuf {
         }
         n_ = bytes;
     }
+    // alloc unless the buffer already has exactly this size (a rebuild reuses it)
+    void ensure(size_t bytes)
+    {
+        if (p_ == nullptr || n_ != bytes) alloc(bytes);
+    }
     void release()
     {
         if (p_) cudaFree(p_);
@@ -224,14 +229,28 @@ struct EpsDivDivOp : Operator {
     int    tile_y = 0, chunk_x = 0;
 
     // free slip on both boundaries: orthonormal rotation modes (3 modes x 3 components x nodes, in
-    // `precision`) and the scratch of the penalty dst += eps sum_i (n_i^T src) n_i
-    DevBuf pen_modes, pen_scratch;
+    // `precision`) and the scratch of the penalty dst += eps sum_i (n_i^T src) n_i; pen_modes32 is the FP32
+    // copy an FP64 operator uses for FP32 applies (prepare_fp32)
+    DevBuf pen_modes, pen_modes32, pen_scratch;
 
     bool   stored = false;
-    DevBuf mats;              // FP64 unbaked element matrices [342][cells]
-    DevBuf baked64, baked32;  // boundary-baked copies (built lazily)
+    DevBuf mats;              // FP64 unbaked element matrices [342][cells] ([342][sel_count] when selective)
+    DevBuf baked64, baked32;  // boundary-baked copies (built lazily; of sel_delta when selective)
     int    baked_bc[2]   = {-1, -1};
     bool   baked32_valid = false;
+
+    // Selective storage (OperatorStoredMatrixMode::Selective, local_matrix_storage.hpp:22-166; the slow path's
+    // choice per cell, epsilon_divdiv_kerngen.hpp:1047-1060): GCA matrices on the cells whose coarsest
+    // ancestor is marked, the on-the-fly operator of k on all others. mats holds the GCA matrices of the
+    // sel_count marked cells (slot s = cell sel_cells[s], sel_slot the inverse map, -1 unmarked); sel_delta
+    // holds mats minus the element matrices of k on those cells. The apply is the matrix-free kernel over every
+    // cell plus sel_delta (baked) over the slots, which equals the per-cell choice because the boundary
+    // treatment and the diagonal mode are linear in the matrix. k32: FP32 copy of k for FP32 applies.
+    bool   selective = false;
+    bool   sel_built = false;
+    int    sel_level_range = 0;
+    int    sel_count       = 0;
+    DevBuf sel_cells, sel_slot, sel_delta, k32;
 
     int  src_components() const override { return 3; }
     int  dst_components() const override { return 3; }
@@ -249,7 +268,16 @@ struct EpsDivDivOp : Operator {
     // stored-matrix helpers
     void ensure_baked(bool need32, cudaStream_t st);
     void set_stored_matrices_from_coefficient(cudaStream_t st);  // element matrices of this level
-    int64_t mats_values() const;
+    int64_t mats_values() const;  // FP64 values of mats
+    // selective storage: cells whose ancestor level_range levels down is marked in marks_dev (one byte per cell
+    // of that level) get stored matrices once a GCA build fills them (synchronous)
+    void set_selective(const uint8_t* marks_dev, int level_range, cudaStream_t st);
+    void finish_selective(cudaStream_t st);  // after the build: the correction sel_delta
+    void materialize_full(cudaStream_t st);  // selective -> full storage (unmarked cells get element matrices)
+    // the matrix of every cell (stored, GCA or element matrix) into out [342][cells], unbaked
+    void effective_matrices(DevBuf& out, cudaStream_t st) const;
+    // FP32 applies of an FP64 operator: FP32 coefficient and penalty modes (synchronous, before capture)
+    void prepare_fp32(cudaStream_t st);
 };
 // TwoGridGCA (gca.hpp:41-531): coarse.mats = sum P^T A_fine P with A_fine the
 // fine operator's stored matrices or its on-the-fly Neumann element matrices.

@@ -153,6 +153,10 @@ def load(path: str = LIB_PATH):
         "tn_vec_rotate_normal_tangential": ([vp, i, i, vpp, i, i, vp], i),
         "tn_vec_freeslip_project": ([vp, i, i, vpp, i, vp], i),
         "tn_stokes_rhs_enforce": ([vp, i, i, i, i, vpp, vp], i),
+        "tn_gca_mark_elements": ([vp, i, i, vp, vp, vp], i),
+        "tn_operator_set_selective_matrices": ([vp, i, vp, vp], i),
+        "tn_operator_stored_cells": ([vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)], i),
+        "tn_solver_level_storage": ([vp, i, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -387,6 +391,18 @@ class EpsDivDiv(Operator):
     def set_stored_matrix_mode(self, mode=STORED_FULL, stream=None):
         _check(load().tn_operator_set_stored_matrix_mode(self._h, mode, _stream(stream)))
 
+    def set_selective_matrices(self, level_range: int, marks, stream=None):
+        """Selective storage (tn_operator_set_selective_matrices): marks is a uint8 device tensor over the cells of
+        the level level_range levels coarser, as gca_mark_elements returns it."""
+        _check(load().tn_operator_set_selective_matrices(self._h, level_range, ctypes.c_void_p(marks.data_ptr()),
+                                                         _stream(stream)))
+
+    def stored_cells(self):
+        """(cells with stored matrices, device bytes of the stored matrices)."""
+        n, b = ctypes.c_int64(), ctypes.c_int64()
+        _check(load().tn_operator_stored_cells(self._h, ctypes.byref(n), ctypes.byref(b)))
+        return n.value, b.value
+
     def local_matrices(self):
         """(10, nl-1, nl-1, nr-1, 2, 18, 18) stored matrices (host)."""
         import numpy as np
@@ -400,6 +416,19 @@ class EpsDivDiv(Operator):
 def gca_build(fine: EpsDivDiv, coarse: EpsDivDiv, stream=None, interpolation=0, tensor_cores=True):
     """TwoGridGCA: coarse receives sum P^T A_fine P (tn_gca_build_interpolated)."""
     _check(load().tn_gca_build_interpolated(fine._h, coarse._h, interpolation, int(tensor_cores), _stream(stream)))
+
+
+def gca_mark_elements(shell: Shell, level: int, level_range: int, k, stream=None):
+    """GCAElementsCollector on the nodal coefficient k of `level`: a uint8 tensor over the cells of level
+    level - level_range, 1 where a descendant wedge's reference-coordinate gradient of k exceeds 10."""
+    import torch
+
+    level = level % shell.num_levels
+    nl, nr = shell.dims(level - level_range)
+    marks = torch.empty((10, nl - 1, nl - 1, nr - 1), dtype=torch.uint8, device=k.device)
+    _check(load().tn_gca_mark_elements(shell.handle, level, level_range, ctypes.c_void_p(k.data_ptr()),
+                                       ctypes.c_void_p(marks.data_ptr()), _stream(stream)))
+    return marks
 
 
 def random_vector(shell: Shell, level: int, ncomp: int, seed: int, dtype=None, stream=None):
@@ -662,6 +691,12 @@ class _Solver:
         out = np.zeros((10, nl - 1, nl - 1, nr - 1, 2, 18, 18))
         _check(load().tn_solver_level_matrices(self._h, level, out.ctypes.data))
         return out
+
+    def level_storage(self, level):
+        """(cells with stored matrices, device bytes of the stored matrices) of hierarchy level `level`."""
+        n, b = ctypes.c_int64(), ctypes.c_int64()
+        _check(load().tn_solver_level_storage(self._h, level, ctypes.byref(n), ctypes.byref(b)))
+        return n.value, b.value
 
 
 def _opt_ptr(eta):

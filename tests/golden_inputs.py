@@ -20,6 +20,16 @@ FGMRES_CASES = {
 }
 POWER_SEED = 12345  # the product's default power-iteration seed; level l uses POWER_SEED + 7919 * l
 
+# adaptive GCA (gca = 2): viscosity contrast 1e4 so that GCAElementsCollector marks part of the coarsest cells
+SELECTIVE = dict(level=4, num_levels=3, seed=3, contrast=1e4, scale=1.0, bcs=(1, 1), fgmres_seed=4, max_it=30)
+# The Stokes solve of the adaptive fixture: at contrast 1e4 the coarsest PCG(50, 1e-6) stops at its iteration
+# limit, where two implementations' rounding drifts apart; contrast 10 scaled by 30 marks 94 of the 640 coarsest
+# cells and the coarsest CG converges in about 35 iterations.
+SELECTIVE_FGMRES = dict(level=4, num_levels=3, seed=3, contrast=10.0, scale=30.0, bcs=(1, 1), fgmres_seed=4,
+                        max_it=40)
+# (level, level_range, viscosity seed, contrast) of the marking fixtures
+MARK_CASES = [(4, 2, 3, 1e4), (4, 3, 5, 3e3), (3, 2, 6, 1e4), (5, 3, 9, 1e5)]
+
 
 def checksum(a) -> float:
     a = np.asarray(a, np.float64).ravel()
@@ -67,3 +77,27 @@ def stokes_case(level, num_levels, bcs, seed, max_it, rtol):
     return dict(level=level, num_levels=num_levels, bcs=bcs, shell=sh, k=k, f=f,
                 b=np.concatenate([f.ravel(), np.zeros(shp.scalar_shape).ravel()]),
                 k_schur=1.0 / O.inject(shp, k), starts=starts, max_it=max_it, rtol=rtol)
+
+
+def selective_case(c=None):
+    """Inputs of the adaptive-GCA fixtures (SELECTIVE unless given): fine shell and viscosity, the injected
+    viscosity of every coarser level (the rediscretised operators' coefficient), one seeded velocity per level,
+    the Stokes right-hand side and the power-iteration start vectors."""
+    c = SELECTIVE if c is None else c
+    lat, nlev = c["level"], c["num_levels"]
+    sh = O.Shell(lat)
+    shp = sh.coarser()
+    k = c["scale"] * smooth_viscosity(sh, c["seed"], c["contrast"])
+    shells = [sh]
+    for _ in range(nlev - 1):
+        shells.insert(0, shells[0].coarser())
+    k_levels = [None] * nlev
+    k_levels[-1] = k
+    for l in range(nlev - 2, -1, -1):
+        k_levels[l] = O.inject(shells[l], k_levels[l + 1])
+    u = [consistent(shells[l], O.seeded_normal(shells[l].vec_shape, 70 + l)) for l in range(nlev)]
+    f = stokes_rhs(sh, c["fgmres_seed"], c["bcs"])
+    starts = [O.seeded_uniform(shells[l], 3, POWER_SEED + 7919 * l) for l in range(nlev)]
+    return dict(shell=sh, shells=shells, k=k, k_levels=k_levels, u=u, f=f, starts=starts,
+                b=np.concatenate([f.ravel(), np.zeros(shp.scalar_shape).ravel()]),
+                k_schur=1.0 / O.inject(shp, k), **c)

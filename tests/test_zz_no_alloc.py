@@ -1,6 +1,6 @@
 """The static-scratch divergence entry point (tn_divergence_apply_noalloc):
 the same result as the operator path on two calls in a row, no change in the
-device's free memory across the calls, and a clear error beyond its scratch
+device's free memory or in torch's caching pool across the calls, and a clear error beyond its scratch
 limit. Kept in the last-collected file so it also runs after every other test."""
 import numpy as np
 import pytest
@@ -33,10 +33,18 @@ def test_noalloc_divergence_matches_operator(cuda, level, bcs, dtype):
         B.apply(u, ref)
         out = torch.full(shp.scalar_shape, float("nan"), dtype=dt, device=cuda)
         torch.cuda.synchronize()
-        free0 = torch.cuda.mem_get_info()[0]
-        T.divergence_apply_noalloc(g, 1, u, out, bc_cmb=bcs[0], bc_surface=bcs[1])
-        torch.cuda.synchronize()
-        assert torch.cuda.mem_get_info()[0] == free0
+        # torch's own pool first (an allocation it would serve without a new cudaMalloc), then the device's
+        # free memory; the device figure may drift with other processes, so it is retried before failing
+        alloc0, reserved0 = torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
+        for attempt in range(3):
+            free0 = torch.cuda.mem_get_info()[0]
+            T.divergence_apply_noalloc(g, 1, u, out, bc_cmb=bcs[0], bc_surface=bcs[1])
+            torch.cuda.synchronize()
+            if torch.cuda.mem_get_info()[0] == free0:
+                break
+        else:
+            pytest.fail("device free memory changed across three calls")
+        assert torch.cuda.memory_allocated() == alloc0 and torch.cuda.memory_reserved() == reserved0
         a, b = out.double().cpu().numpy(), ref.double().cpu().numpy()
         tol = 1e-13 if dtype == "f64" else 1e-5
         assert np.abs(a - b).max() <= tol * np.abs(b).max()

@@ -334,7 +334,7 @@ int tn_operator_copy_local_matrices(tn_operator* op, double* mats_host);
  * preconditioner (FGMRESOptions, fgmres.hpp:13-28; IterativeSolverParameters;
  * StokesSolverParameters, apps/mantlecirculation/src/parameters.hpp:154-184). */
 typedef struct tn_solver_options {
-    int      restart;                   /* FGMRES(m), 1..64 (30) */
+    int      restart;                   /* FGMRES(m), 1..128 (30) */
     int      max_iterations;            /* outer iterations (300) */
     double   relative_tolerance;        /* 1e-8 */
     double   absolute_tolerance;        /* 1e-12 */

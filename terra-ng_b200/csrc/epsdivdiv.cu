@@ -183,9 +183,9 @@ template <typename T, int CPL>
 __host__ __device__ inline SmemLayout<T> edd_smem_layout(int nr, int ty, int cx, int nfields)
 {
     SmemLayout<T> L;
-    L.bar_off       = 0;
+    L.bar_off       = 0;  // 3 mbarriers, then the element offsets of the staged rows (3 slots x 4 fields, int)
     L.rowcap        = static_cast<uint32_t>(((static_cast<size_t>(ty + 2) * nr * sizeof(T) + 16) + 15) / 16 * 16);
-    L.ring_off      = 64;
+    L.ring_off      = 128;
     L.geo_off       = L.ring_off + static_cast<size_t>(3) * nfields * L.rowcap;
     L.nrm_off       = L.geo_off + static_cast<size_t>(ty + 1) * (cx + 1) * 20 * sizeof(T);
     L.bco_off       = L.nrm_off + static_cast<size_t>(ty + 1) * (cx + 1) * 12 * sizeof(T);
@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 
     const SmemLayout<T> L   = edd_smem_layout<T, CPL>(nr, ty, cx, nfields);
     uint64_t*           bar = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    int*                row_off = reinterpret_cast<int*>(smem + L.bar_off + 32);  // [slot][field]
     unsigned char*      ring = smem + L.ring_off;
     T*                  geo  = reinterpret_cast<T*>(smem + L.geo_off);
     T*                  nrms = reinterpret_cast<T*>(smem + L.nrm_off);
@@ -224,14 +225,9 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
     const int nsteps = cx + 1;  // cell columns xs-1 .. xs+cx-1
     const T*  fields[4] = {A.src[0], A.src[1], A.src[2], A.k};
 
-    // Element offset (0..15 bytes / sizeof(T)) of the first staged element of
-    // node row xr in the bulk-copied buffer of field f (each field may sit at a
-    // different alignment).
-    auto row_offset = [&](int f, int xr) -> int {
-        const int64_t  e0 = node_index(nl, nr, d, xr, ylo, 0);
-        const uint64_t a  = reinterpret_cast<uint64_t>(fields[f] + e0);
-        return static_cast<int>((a & 15u) / sizeof(T));
-    };
+    // The issuing thread records, per ring slot and field, the element offset (0..15 bytes / sizeof(T)) of the
+    // first staged element in the bulk-copied buffer (each field may sit at a different alignment); the
+    // mbarrier's release / acquire makes it visible with the row.
     auto issue_row = [&](int i) {
         const int xr   = xs - 1 + i;
         const int slot = i % 3;
@@ -249,6 +245,7 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
             const uint32_t off = static_cast<uint32_t>(a - al);
             bytes[f]           = (off + static_cast<uint32_t>(ncols) * nr * sizeof(T) + 15u) & ~15u;
             srcp[f]            = reinterpret_cast<const T*>(al);
+            row_off[slot * 4 + f] = static_cast<int>(off / sizeof(T));
             total += bytes[f];
         }
         mbar_arrive_expect_tx(&bar[slot], total);
@@ -351,8 +348,8 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
         int offA[4], offB[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            offA[f] = (f < nfields && x >= 0 && x < nl) ? row_offset(f, x) : 0;
-            offB[f] = (f < nfields && x + 1 >= 0 && x + 1 < nl) ? row_offset(f, x + 1) : 0;
+            offA[f] = (f < nfields && x >= 0 && x < nl) ? row_off[(i % 3) * 4 + f] : 0;
+            offB[f] = (f < nfields && x + 1 >= 0 && x + 1 < nl) ? row_off[((i + 1) % 3) * 4 + f] : 0;
         }
         const T*  rowA = reinterpret_cast<const T*>(ring + static_cast<size_t>(i % 3) * nfields * L.rowcap);
         const T*  rowB = reinterpret_cast<const T*>(ring + static_cast<size_t>((i + 1) % 3) * nfields * L.rowcap);
@@ -570,13 +567,14 @@ __global__ void __launch_bounds__(32 * MaxWarps<T>::value) epsdivdiv_kernel(EddA
 
         const int yn = yc;  // node line owned by warp w (w >= 1)
         if (ok && w >= 1 && i >= 1 && x < nl && yn < nl) {
-            const T* slot_p = xch + (static_cast<size_t>(i & 1) * nwarps + (w - 1)) * 3 * (CPL + 1) * 32 + lane;
+            const T*  slot_p = xch + (static_cast<size_t>(i & 1) * nwarps + (w - 1)) * 3 * (CPL + 1) * 32 + lane;
+            const int obase  = ((d * nl + x) * nl + yn) * nr;  // 32-bit: the host limits a level to 2^31 nodes
 #pragma unroll
             for (int j = 0; j <= CPL; ++j) {
                 const int rn = (j < CPL) ? lane + 32 * j : nr - 1;
                 const bool own = (j < CPL) ? (rn < nr - 1) : (lane == lane_top);
                 if (!own) continue;
-                const int64_t id = node_index(nl, nr, d, x, yn, rn);
+                const int id = obase + rn;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     const T v = keep[j][c] + slot_p[(j * 3 + c) * 32];
@@ -688,6 +686,7 @@ int epsdivdiv_apply(const EddLaunch<T>& p, cudaStream_t stream)
         }
     }
     if (a.ty + 1 > MaxWarps<T>::value) return -4;
+    if (10LL * p.nl * p.nl * p.nr >= (1LL << 31)) return -6;  // the kernel indexes nodes in 32 bits
     return launch<T>(a, p.diagonal, stream);
 }
 

@@ -613,7 +613,7 @@ StokesSolver::StokesSolver(const Shell* sh, int vlevel, const double* eta_nodal,
         throw Error(kErrArg, "exactly one of eta_nodal / eta_cell must be given");
     if (vlevel < 1) throw Error(kErrArg, "the velocity level needs a pressure level below it");
     if (o.restart < 1 || o.restart > kMaxAxpy || o.restart + 2 > Scratch::kScalars || o.max_iter < 0)
-        throw Error(kErrArg, "FGMRES restart must be in 1..64");
+        throw Error(kErrArg, "FGMRES restart must be in 1..128");
     if (eta_cell && !k_schur) throw Error(kErrArg, "a cell viscosity needs the Schur coefficient k_schur");
     const DeviceLevel& Lu = sh->level(vlevel);
     const DeviceLevel& Lp = sh->level(vlevel - 1);

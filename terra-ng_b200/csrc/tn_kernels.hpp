@@ -257,7 +257,7 @@ struct RedScratch {
     double*   partials = nullptr;
     unsigned* counter  = nullptr;
 };
-constexpr int kMaxAxpy = 64;
+constexpr int kMaxAxpy = 128;  // FGMRES restart limit (the list is a kernel parameter: 2 KB)
 struct AxpyList {
     const double* z[kMaxAxpy];
     double        y[kMaxAxpy];

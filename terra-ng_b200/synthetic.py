@@ -165,19 +165,26 @@ def cell_viscosity_radial_jump(shell: "T.Shell", level: int, seed: int = 1, cont
     return eta
 
 
-def schur_coefficient_from_cells(shell: "T.Shell", velocity_level: int, eta_cell):
-    """Nodal 1/eta on the pressure level (velocity_level - 1) for a per-cell
-    viscosity: at each pressure node, the mean of 1/eta over the fine cells
-    touching it, averaged over all copies of an interface node."""
+def schur_coefficient_from_cells(shell: "T.Shell", velocity_level: int, eta_cell, mode: str = "inverse_mean"):
+    """Nodal Schur-block coefficient k = 1/eta on the pressure level (velocity_level - 1) for a per-cell
+    viscosity, from the fine cells touching each pressure node (over all copies of an interface node).
+
+    mode "inverse_mean" (default): k = 1 / mean(eta). mode "mean_inverse": k = mean(1 / eta). The two differ
+    where a node touches cells of very different viscosity: the first follows the stiff cells, the second the
+    soft ones. With cell-wise jumps of 1e4 (log-uniform lateral blocks at level 5) the lumped-mass Schur block
+    built from "inverse_mean" takes FGMRES(30) to 1e-4 in 192 iterations against 657 for "mean_inverse", and
+    with FGMRES(128) to 1e-8 in 1247 iterations, where "mean_inverse" still stands at 2e-7 after 2000."""
+    if mode not in ("inverse_mean", "mean_inverse"):
+        raise ValueError(mode)
     nlf = eta_cell.shape[1] + 1
     nrf = eta_cell.shape[3] + 1
-    inv = 1.0 / eta_cell
+    val = eta_cell if mode == "inverse_mean" else 1.0 / eta_cell
     acc = np.zeros((10, nlf, nlf, nrf))
     cnt = np.zeros((10, nlf, nlf, nrf))
     for dx in (0, 1):
         for dy in (0, 1):
             for dr in (0, 1):
-                acc[:, dx:nlf - 1 + dx, dy:nlf - 1 + dy, dr:nrf - 1 + dr] += inv
+                acc[:, dx:nlf - 1 + dx, dy:nlf - 1 + dy, dr:nrf - 1 + dr] += val
                 cnt[:, dx:nlf - 1 + dx, dy:nlf - 1 + dy, dr:nrf - 1 + dr] += 1.0
     cls, ncls = shell.duplicate_classes(velocity_level)
     flat_a = acc.reshape(10 * nlf * nlf, nrf)
@@ -187,5 +194,6 @@ def schur_coefficient_from_cells(shell: "T.Shell", velocity_level: int, eta_cell
         m = np.where(cl == k)[0]
         flat_a[m] = flat_a[m].sum(axis=0)
         flat_c[m] = flat_c[m].sum(axis=0)
-    node = flat_a.reshape(acc.shape) / flat_c.reshape(cnt.shape)
+    mean = flat_a.reshape(acc.shape) / flat_c.reshape(cnt.shape)
+    node = 1.0 / mean if mode == "inverse_mean" else mean
     return np.ascontiguousarray(node[:, ::2, ::2, ::2])

@@ -6,16 +6,12 @@ an N(0,1) body force; one operator apply against the oracle (1e-12) and a
 CG solve preconditioned by the GMG V(2,2) with Chebyshev order 3 to 1e-8,
 whose residual history equals the oracle's.
 
-Adjoint with per-cell block viscosity (level 4 here): log-uniform [1, 10^2]
-lateral blocks in a smooth background (contrast up to ~300), J = 1/2 ||u -
-u_obs||^2 with u_obs from a perturbed viscosity; the adjoint gradient against
-central differences along random element directions (1e-6 relative; step
-1e-5 with forward solves to 1e-13, the step test_gpu_adjoint.py explains).
-The finite-difference check needs forward solves to ~1e-13; with 10^4 jumps
-between cells the FGMRES / block-preconditioner iteration (the reference's
-algorithm) needs far more than a test's budget of iterations to get there
-(about 900 iterations reach 1e-6 at level 4), so the test uses a contrast at
-which it converges in a few hundred."""
+Adjoint with per-cell block viscosity: at level 4 with log-uniform [1, 10^2] lateral blocks in a smooth
+background (contrast up to ~300), and at level 5 with [1, 10^4] blocks (configuration 3, contrast 8e4); J = 1/2
+||u - u_obs||^2 with u_obs from a perturbed viscosity; the adjoint gradient against central differences along
+random element directions to 1e-6 relative (level 4: step 1e-5, 3 directions; level 5: step 1e-6, 32 directions).
+At the 10^4 contrast the solves use FGMRES(128) and the Schur coefficient 1/mean(eta) of the cells around each
+pressure node, with which they reach 1e-13."""
 import numpy as np
 import pytest
 
@@ -113,6 +109,72 @@ def test_block_viscosity_adjoint_gradient(cuda):
         fd = (J(theta + h * d) - J(theta - h * d)) / (2 * h)
         ad = float(np.sum(gnp * d))
         assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+
+
+def test_configuration3_adjoint_gradient_level5(cuda):
+    """Configuration 3: level 5, per-cell viscosity from log-uniform [1, 1e4] lateral blocks in a smooth background
+    (contrast 8e4), no-slip CMB / free-slip surface, J = 1/2 sum_owned |u - u_obs|^2. The forward and adjoint
+    solves reach 1e-13 (FGMRES(128), Schur coefficient 1/mean(eta)), and the adjoint gradient agrees with central
+    differences along 32 random element directions at step 1e-6 to 1e-6 relative. The perturbed solves start from
+    the unperturbed solution and reduce their residual by 2e-9; the difference J(+) - J(-) is summed as
+    1/2 (u+ - u-).(u+ + u- - 2 u_obs) with exact rounding (math.fsum), so no cancellation of two J values enters."""
+    import math
+
+    import torch
+
+    level, nlev, bcs = 5, 4, (1, 2)
+    g = T.Shell(level, num_levels=nlev)
+    fine = nlev - 1
+    eta = S.cell_viscosity_blocks(g, fine, seed=3, tiles=4, fraction=0.3, max_log10=4.0,
+                                  background_log_amplitude=0.5 * np.log(10.0))
+    assert eta.max() / eta.min() > 1e4
+    theta = np.log(eta)
+    ks = _t(S.schur_coefficient_from_cells(g, fine, eta))
+    f = S.buoyancy_rhs(g, fine, S.temperature(g, fine, seed=2), *bcs)
+    nlp, nrp = g.dims(fine - 1)
+    own = torch.tensor(g.ownership(fine), device=cuda).bool()
+
+    def solve(th, rtol, x0=None, max_iterations=4000):
+        s = T.StokesSolver(g, eta_cell=_t(np.exp(th)), k_schur=ks, bc_cmb=bcs[0], bc_surface=bcs[1], restart=128,
+                           coarse_solver=T.COARSE_DENSE, mixed_precision=1, relative_tolerance=rtol,
+                           absolute_tolerance=0.0, max_iterations=max_iterations, project_pressure_mean=1,
+                           normalize_pressure=0)
+        x = [torch.zeros_like(f[0]) for _ in range(3)]
+        x.append(torch.zeros((10, nlp, nlp, nrp), dtype=torch.float64, device=cuda))
+        if x0 is not None:
+            for t, t0 in zip(x, x0):
+                t.copy_(t0)
+        ok = s.solve(x, [f[c].contiguous() for c in range(3)] + [torch.zeros_like(x[3])])
+        return s, x, ok
+
+    rng = np.random.default_rng(5)
+    _, xo, ok = solve(theta + 0.1 * rng.standard_normal(theta.shape), 1e-10)
+    assert ok
+    u_obs = [xo[c] for c in range(3)]
+    s, x_base, ok = solve(theta, 1e-13)
+    assert ok
+    grad = torch.zeros(theta.shape, dtype=torch.float64, device=cuda)
+    assert s.misfit_gradient(x_base, u_obs, grad)
+    assert s.result()[1] <= 1e-13
+    gnp = grad.cpu().numpy()
+    del s
+
+    def delta_j(up, um):
+        terms = [((up[c] - um[c]) * (up[c] + um[c] - 2 * u_obs[c]))[own].cpu().numpy() for c in range(3)]
+        return 0.5 * math.fsum(np.concatenate(terms))
+
+    h, errs = 1e-6, []
+    drng = np.random.default_rng(6)
+    for _ in range(32):
+        d = drng.standard_normal(theta.shape)
+        xs = []
+        for sgn in (1.0, -1.0):
+            _, x, ok = solve(theta + sgn * h * d, 2e-9, x_base, 3000)
+            xs.append(x)
+        fd = delta_j(xs[0], xs[1]) / (2 * h)
+        ad = math.fsum((gnp * d).ravel())
+        errs.append(abs(fd - ad) / abs(ad))
+    assert max(errs) <= 1e-6, errs
 
 
 @pytest.mark.parametrize("bcs", [(1, 1), (1, 2), (2, 2)])

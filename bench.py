@@ -76,7 +76,7 @@ def _args():
                          "one is timed once beside it")
     ap.add_argument("--workload", default="solve", choices=["solve", "apply-f32", "apply-f64", "coupling",
                                                              "precondition", "adjoint-L5", "solve-L7", "gca-build",
-                                                             "gca-modes"],
+                                                             "gca-modes", "solve-profile"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
                          "apply; coupling: the L6 B and B^T applies (FP64); precondition: one application of the "
                          "L6 mixed-precision block preconditioner; gca-build: the Galerkin coarse operators of the "
@@ -514,6 +514,45 @@ def run_gca_modes(a):
                                              "of contrast 1e6 (benchmark field, log-amplitude ln(1000)), FGMRES(30) "
                                              "to 1e-8 with the FP32 V-cycle and the dense coarsest solve"},
                       "modes": out}), flush=True)
+
+
+def run_solve_profile(a):
+    """The level-6 benchmark solve for launch lists: after one warm-up solve each, one mixed-precision and one FP64
+    solve inside the NVTX ranges "mixed_solve" and "fp64_solve" (ncu --nvtx --nvtx-include "mixed_solve/")."""
+    import torch
+
+    import synthetic as S
+    import terra_b200 as T
+
+    shell = T.Shell(LEVEL, num_levels=NUM_LEVELS)
+    fine = NUM_LEVELS - 1
+    eta = torch.tensor(S.viscosity(shell, fine, seed=SEED_ETA), device="cuda")
+    f = S.buoyancy_rhs(shell, fine, S.temperature(shell, fine, seed=SEED_TEMP), *BCS)
+    x = _stokes_vectors(torch, shell, fine, "cuda")
+    b = [f[c].contiguous() for c in range(3)] + [torch.zeros_like(x[3])]
+    out = {}
+    for name, mixed in (("mixed", 1), ("fp64", 0)):
+        sol = T.StokesSolver(shell, eta=eta, bc_cmb=BCS[0], bc_surface=BCS[1], mixed_precision=mixed,
+                             coarse_solver=T.COARSE_DENSE if a.coarse == "dense" else T.COARSE_PCG,
+                             relative_tolerance=1e-8, absolute_tolerance=0.0, max_iterations=3000,
+                             project_pressure_mean=1)
+        for t in x:
+            t.zero_()
+        sol.solve(x, b)
+        for t in x:
+            t.zero_()
+        torch.cuda.synchronize()
+        l0 = T.kernel_launch_count()
+        torch.cuda.nvtx.range_push(f"{name}_solve")
+        dt, _ = _timed(torch, lambda: sol.solve(x, b))
+        torch.cuda.nvtx.range_pop()
+        its, rr, conv = sol.result()
+        out[name] = {"s": dt, "iterations": its, "relative_residual": rr, "converged": conv,
+                     "launches": T.kernel_launch_count() - l0}
+        del sol
+    print(json.dumps({"metric": "L6 Stokes solve (launch-list workload)", "unit": "s/solve", "n_gpus": 1,
+                      "higher_is_better": False, "data": "synthetic", "config": {"workload": WORKLOAD},
+                      "solves": out}), flush=True)
 
 
 def run_precondition(a):
@@ -982,6 +1021,8 @@ def main():
         run_gca_build(a)
     elif a.workload == "gca-modes":
         run_gca_modes(a)
+    elif a.workload == "solve-profile":
+        run_solve_profile(a)
     elif a.workload == "adjoint-L5":
         run_adjoint_l5(a)
     elif a.workload == "solve-L7":

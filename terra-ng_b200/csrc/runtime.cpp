@@ -267,14 +267,7 @@ void EpsDivDivOp::prepare_fp32(cudaStream_t st)
             throw Error(kErrCuda, "conversion launch failed");
         k32 = std::move(b);
     }
-    if (penalty_active() && pen_modes32.get() == nullptr) {
-        prepare_penalty(st);
-        const int64_t n = 9 * lvl().nodes();
-        DevBuf        b(sizeof(float) * static_cast<size_t>(n));
-        if (convert_f64_to_f32(n, pen_modes.as<double>(), b.as<float>(), st) != 0)
-            throw Error(kErrCuda, "conversion launch failed");
-        pen_modes32 = std::move(b);
-    }
+    prepare_penalty(st);
     cuda_check(cudaStreamSynchronize(st), "prepare fp32");
 }
 
@@ -349,61 +342,43 @@ void gca_coarsen(const EpsDivDivOp& fine, EpsDivDivOp& coarse, cudaStream_t st, 
 
 void EpsDivDivOp::prepare_penalty(cudaStream_t st)
 {
-    if (!penalty_active() || pen_modes.get() != nullptr) return;
+    if (!penalty_active() || pen_ready) return;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cuda_check(cudaStreamIsCapturing(st, &cap), "capture status");
     if (cap != cudaStreamCaptureStatusNone)
         throw Error(kErrState, "the free-slip null-space modes must be built before stream capture");
-    const DeviceLevel& L  = lvl();
-    const int64_t      n  = L.nodes();
-    const uint8_t*     ow = L.owned_lat.as<uint8_t>();
-    double*            red = shell->red.as<double>();
-    DevBuf             m64(sizeof(double) * 9 * static_cast<size_t>(n));
-    if (null_space_modes_raw(n, L.nr(), L.coords<double>(), L.radii<double>(), m64.as<double>(), st) != 0)
-        throw Error(kErrCuda, "null-space mode launch failed");
-    auto mode = [&](int a, double** out) {
-        for (int d = 0; d < 3; ++d) out[d] = m64.as<double>() + (static_cast<int64_t>(a) * 3 + d) * n;
+    const DeviceLevel& L = lvl();
+    pen_scratch.alloc(sizeof(double) * (penalty_partials_size() + 8));
+    double* ps = pen_scratch.as<double>();
+    if (penalty_gram(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), L.coords<double>(), L.radii<double>(), ps + 8, ps,
+                     st) != 0)
+        throw Error(kErrCuda, "null-space Gram launch failed");
+    double g6[6];
+    cuda_check(cudaMemcpyAsync(g6, ps, sizeof(g6), cudaMemcpyDeviceToHost, st), "Gram readback");
+    cuda_check(cudaStreamSynchronize(st), "Gram sync");
+    const double G[3][3] = {{g6[0], g6[1], g6[2]}, {g6[1], g6[3], g6[4]}, {g6[2], g6[4], g6[5]}};
+    auto         inner   = [&](const double* a, const double* b) {
+        double v = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) v += a[i] * G[i][j] * b[j];
+        return v;
     };
-    auto dot = [&](int a, int b) {
-        double* ma[3];
-        double* mb[3];
-        mode(a, ma);
-        mode(b, mb);
-        const double* ca[3] = {ma[0], ma[1], ma[2]};
-        const double* cb[3] = {mb[0], mb[1], mb[2]};
-        if (masked_dot<double>(n, L.nr(), 3, ow, ca, cb, red, red + 8, st) != 0)
-            throw Error(kErrCuda, "dot launch failed");
-        double h = 0.0;
-        cuda_check(cudaMemcpyAsync(&h, red, sizeof(double), cudaMemcpyDeviceToHost, st), "dot readback");
-        cuda_check(cudaStreamSynchronize(st), "dot sync");
-        return h;
-    };
-    // modified Gram-Schmidt with owned-node dots, then normalisation (epsilon_divdiv_kerngen.hpp:403-440)
+    // modified Gram-Schmidt with owned-node dots, then normalisation (epsilon_divdiv_kerngen.hpp:403-440), on the
+    // coefficients of the modes in the raw basis
+    double C[3][3] = {};
     for (int i = 0; i < 3; ++i) {
-        double* mi[3];
-        mode(i, mi);
-        const double* ci[3] = {mi[0], mi[1], mi[2]};
+        double a[3] = {0.0, 0.0, 0.0};
+        a[i]        = 1.0;
         for (int j = 0; j < i; ++j) {
-            double* mj[3];
-            mode(j, mj);
-            const double* cj[3] = {mj[0], mj[1], mj[2]};
-            const double  c[2]  = {1.0, -dot(i, j)};
-            if (lincomb<double>(n, 3, mi, 0.0, 2, c, ci, cj, nullptr, st) != 0)
-                throw Error(kErrCuda, "lincomb launch failed");
+            const double d = inner(a, C[j]);
+            for (int q = 0; q < 3; ++q) a[q] -= d * C[j][q];
         }
-        const double inv = 1.0 / std::sqrt(dot(i, i));
-        if (lincomb<double>(n, 3, mi, 0.0, 1, &inv, ci, nullptr, nullptr, st) != 0)
-            throw Error(kErrCuda, "lincomb launch failed");
+        const double inv = 1.0 / std::sqrt(inner(a, a));
+        for (int q = 0; q < 3; ++q) C[i][q] = a[q] * inv;
     }
-    if (precision == 0) {
-        pen_modes = std::move(m64);
-    } else {
-        pen_modes.alloc(sizeof(float) * 9 * static_cast<size_t>(n));
-        if (convert_f64_to_f32(9 * n, m64.as<double>(), pen_modes.as<float>(), st) != 0)
-            throw Error(kErrCuda, "conversion launch failed");
-        cuda_check(cudaStreamSynchronize(st), "mode conversion");
-    }
-    pen_scratch.alloc(sizeof(double) * (penalty_partials_size() + 4));
+    for (int i = 0; i < 3; ++i)
+        for (int q = 0; q < 3; ++q) pen_coef.c[3 * i + q] = C[i][q];
+    pen_ready = true;
 }
 
 template <typename T>
@@ -411,14 +386,10 @@ void EpsDivDivOp::add_penalty(const T* const* src, T* const* dst, cudaStream_t s
 {
     if (!penalty_active() || diagonal) return;
     prepare_penalty(st);
-    const DeviceLevel& L      = lvl();
-    double*            ps     = pen_scratch.as<double>();
-    const bool         fp32_of_fp64 = std::is_same<T, float>::value && precision == 0;
-    if (fp32_of_fp64 && pen_modes32.get() == nullptr)
-        throw Error(kErrState, "FP32 apply of an FP64 operator: prepare_fp32 was not called");
-    const T* modes = fp32_of_fp64 ? pen_modes32.as<T>() : pen_modes.as<T>();
-    if (penalty_apply<T>(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), src, dst, modes, kPenaltyEpsilon,
-                         ps + 4, ps, st) != 0)
+    const DeviceLevel& L  = lvl();
+    double*            ps = pen_scratch.as<double>();
+    if (penalty_apply<T>(L.nodes(), L.nr(), L.owned_lat.as<uint8_t>(), L.coords<T>(), L.radii<T>(), src, dst,
+                         pen_coef, kPenaltyEpsilon, ps + 8, ps, st) != 0)
         throw Error(kErrCuda, "penalty launch failed");
 }
 

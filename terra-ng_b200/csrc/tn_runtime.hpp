@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "tn_boundary.hpp"
 #include "tn_grid.hpp"
 #include "tn_kernels.hpp"
 
@@ -228,10 +229,11 @@ struct EpsDivDivOp : Operator {
     bool   diagonal = false;
     int    tile_y = 0, chunk_x = 0;
 
-    // free slip on both boundaries: orthonormal rotation modes (3 modes x 3 components x nodes, in
-    // `precision`) and the scratch of the penalty dst += eps sum_i (n_i^T src) n_i; pen_modes32 is the FP32
-    // copy an FP64 operator uses for FP32 applies (prepare_fp32)
-    DevBuf pen_modes, pen_modes32, pen_scratch;
+    // free slip on both boundaries: the orthonormal rotation modes as coefficients over the raw modes e_i x X
+    // (evaluated from the coordinates by the kernels) and the scratch of the penalty dst += eps sum_i (n_i^T src) n_i
+    PenaltyCoef pen_coef;
+    bool        pen_ready = false;
+    DevBuf      pen_scratch;
 
     bool   stored = false;
     DevBuf mats;              // FP64 unbaked element matrices [342][cells] ([342][sel_count] when selective)
@@ -262,7 +264,7 @@ struct EpsDivDivOp : Operator {
     void vjp_logeta(const T* const* u, const T* const* lam, T* grad_cell, cudaStream_t st) const;
     // free-slip/free-slip null-space penalty (epsilon_divdiv_kerngen.hpp:324-445, :711-785)
     bool penalty_active() const { return bc_cmb == 2 && bc_surf == 2; }
-    void prepare_penalty(cudaStream_t st);  // builds the modes (synchronous); no-op unless active or built
+    void prepare_penalty(cudaStream_t st);  // orthonormalises the modes (synchronous); no-op unless active or done
     template <typename T>
     void add_penalty(const T* const* src, T* const* dst, cudaStream_t st);
     // stored-matrix helpers
@@ -276,7 +278,7 @@ struct EpsDivDivOp : Operator {
     void materialize_full(cudaStream_t st);  // selective -> full storage (unmarked cells get element matrices)
     // the matrix of every cell (stored, GCA or element matrix) into out [342][cells], unbaked
     void effective_matrices(DevBuf& out, cudaStream_t st) const;
-    // FP32 applies of an FP64 operator: FP32 coefficient and penalty modes (synchronous, before capture)
+    // FP32 applies of an FP64 operator: FP32 coefficient and the penalty set-up (synchronous, before capture)
     void prepare_fp32(cudaStream_t st);
 };
 // TwoGridGCA (gca.hpp:41-531): coarse.mats = sum P^T A_fine P with A_fine the

@@ -415,3 +415,36 @@ def test_velocity_cg_matches_oracle(cuda):
     assert len(ohist) == len(hist)
     assert np.allclose(hist, ohist, rtol=1e-6, atol=1e-13)
     assert rel_err(x.cpu().numpy(), xo) < 1e-7
+
+
+@pytest.mark.parametrize("mixed", [1, 0])
+def test_repeated_solves_stay_within_stated_drift(cuda, mixed):
+    """The Galerkin stored apply and B's scatter add into their outputs with floating-point atomics, so two runs of
+    the same solve need not agree bit for bit. The drift allowed between runs: the same iteration count, residual
+    histories within 1e-4 relative with the FP32 V-cycle and 1e-8 in FP64, and solutions within 1e-10 and 1e-13
+    relative (measured at levels 4 and 5: 1.1e-5 / 1.4e-12 mixed, 2e-10 / 1e-15 FP64)."""
+    import torch
+
+    from golden_inputs import stokes_rhs
+
+    level, nlev = 4, 3
+    sh = O.Shell(level)
+    shp = sh.coarser()
+    k = smooth_viscosity(sh, 3, 100.0)
+    f = stokes_rhs(sh, 4, (1, 2))
+    g = T.Shell(level, num_levels=nlev)
+    runs = []
+    for _ in range(3):
+        s = T.StokesSolver(g, eta=_t(k), bc_cmb=1, bc_surface=2, mixed_precision=mixed, relative_tolerance=1e-8,
+                           absolute_tolerance=0.0, max_iterations=2000, project_pressure_mean=1,
+                           coarse_solver=T.COARSE_DENSE)
+        x = [torch.zeros(sh.scalar_shape, dtype=torch.float64, device=cuda) for _ in range(3)]
+        x.append(torch.zeros(shp.scalar_shape, dtype=torch.float64, device=cuda))
+        b = [_t(f[c]) for c in range(3)] + [torch.zeros_like(x[3])]
+        assert s.solve(x, b)
+        runs.append((np.array(s.history()), np.concatenate([t.cpu().numpy().ravel() for t in x[:3]])))
+    h0, x0 = runs[0]
+    for h, x in runs[1:]:
+        assert len(h) == len(h0)
+        assert np.allclose(h, h0, rtol=1e-4 if mixed else 1e-8, atol=0.0)
+        assert rel_err(x, x0) < (1e-10 if mixed else 1e-13)

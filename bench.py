@@ -83,10 +83,11 @@ def _args():
                                                              "gca-modes", "solve-profile"],
                     help="solve: the L6 Stokes solve (default); apply-*: the standalone L6 fine-level operator "
                          "apply; coupling: the L6 B and B^T applies (FP64); precondition: one application of the "
-                         "L6 mixed-precision block preconditioner; gca-build: the Galerkin coarse operators of the "
-                         "L6 hierarchy on the FP64 tensor cores and as scalar FMAs; adjoint-L5: the L5 misfit gradient with a "
-                         "finite-difference check; solve-L7: the L7 mixed and FP64 solves plus one adjoint "
-                         "gradient")
+                         "L6 mixed-precision block preconditioner; gca-build: the L6 Galerkin hierarchy build, fast "
+                         "against plain scalar and adaptive against full; gca-modes: the L6 solve with full, "
+                         "adaptive and no GCA; solve-profile: one mixed and one FP64 L6 solve inside NVTX ranges; "
+                         "adjoint-L5: the L5 misfit gradient at 1e4 contrast with a finite-difference check; "
+                         "solve-L7: the L7 mixed and FP64 solves plus one adjoint gradient")
     return ap.parse_args()
 
 
@@ -952,7 +953,8 @@ def run_solve_l7(a):
     f = S.buoyancy_rhs(g, fine, S.temperature(g, fine, seed=SEED_TEMP), *bcs)
     t_inputs = time.perf_counter() - t0
     opts = dict(k_schur=ks, bc_cmb=bcs[0], bc_surface=bcs[1], relative_tolerance=1e-8, absolute_tolerance=0.0,
-                max_iterations=2000, restart=30, project_pressure_mean=1, normalize_pressure=0)
+                max_iterations=2000, restart=30, project_pressure_mean=1, normalize_pressure=0,
+                chebyshev_order=CHEB_ORDER, coarse_solver=T.COARSE_DENSE)
     free0 = torch.cuda.mem_get_info(dev)[0]
 
     # observations from a perturbed viscosity (one mixed solve, solver released before the timed ones)

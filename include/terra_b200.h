@@ -211,6 +211,17 @@ int tn_vec_lincomb(tn_shell* shell, int level, int precision, int ncomp, void* c
 int tn_vec_dot(tn_shell* shell, int level, int precision, int ncomp, const void* const* a_dev,
                const void* const* b_dev, double* result, void* stream);
 
+/* A nodal vector of `level` (the VectorQ1Scalar / VectorQ1Vec constructors,
+ * src/terra/linalg/vector_q1.hpp:20-120): ncomp arrays of the level's
+ * (10, nl, nl, nr) nodes in `precision`, zero-filled, 256-byte aligned, their
+ * device pointers written to comps_out. Synchronous. tn_vec_free releases
+ * them (NULL entries are skipped). */
+int  tn_vec_alloc(tn_shell* shell, int level, int precision, int ncomp, void** comps_out);
+void tn_vec_free(int ncomp, void* const* comps);
+/* Waits for everything queued on `stream` (the reference's Kokkos::fence()
+ * after each apply); TN_ERR_CUDA if a launch or copy on it failed. */
+int tn_sync(void* stream);
+
 /* Uniform(-1, 1) values from SplitMix64 of (seed, canonical node, component):
  * the canonical node is the lowest lateral index of the node's duplicate class
  * times nr plus r, so interface duplicates receive equal values. Stands in for

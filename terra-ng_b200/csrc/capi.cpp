@@ -897,6 +897,46 @@ int tn_operator_copy_local_matrices(tn_operator* op, double* mats_host)
     });
 }
 
+int tn_vec_alloc(tn_shell* shell, int level, int precision, int ncomp, void** comps_out)
+{
+    return guarded([&] {
+        need(shell && comps_out, "NULL argument");
+        need(ncomp >= 1 && ncomp <= 4, "ncomp must be 1..4");
+        const size_t esz = precision_size(precision);
+        const auto&  L   = shell->impl->level(level);
+        // padded to 256 bytes so that 16-byte-rounded bulk reads stay inside the allocation
+        const size_t bytes = (esz * static_cast<size_t>(L.nodes()) + 255) / 256 * 256;
+        for (int c = 0; c < ncomp; ++c) comps_out[c] = nullptr;
+        try {
+            for (int c = 0; c < ncomp; ++c) {
+                if (cudaMalloc(&comps_out[c], bytes) != cudaSuccess) {
+                    cudaGetLastError();
+                    comps_out[c] = nullptr;
+                    throw tn::Error(tn::kErrAlloc, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+                }
+                tn::cuda_check(cudaMemset(comps_out[c], 0, bytes), "zero vector");
+            }
+        } catch (...) {
+            for (int c = 0; c < ncomp; ++c)
+                if (comps_out[c]) cudaFree(comps_out[c]);
+            for (int c = 0; c < ncomp; ++c) comps_out[c] = nullptr;
+            throw;
+        }
+    });
+}
+
+void tn_vec_free(int ncomp, void* const* comps)
+{
+    if (!comps) return;
+    for (int c = 0; c < ncomp; ++c)
+        if (comps[c]) cudaFree(comps[c]);
+}
+
+int tn_sync(void* stream)
+{
+    return guarded([&] { tn::cuda_check(cudaStreamSynchronize(as_stream(stream)), "stream synchronize"); });
+}
+
 int tn_vec_random(tn_shell* shell, int level, int precision, int ncomp, uint64_t seed, void* const* comps_dev,
                   void* stream)
 {

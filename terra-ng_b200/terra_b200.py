@@ -114,6 +114,9 @@ def load(path: str = LIB_PATH):
         "tn_vec_lincomb": ([vp, i, i, i, vpp, d, i, dp, vpp, vpp, vpp, vp], i),
         "tn_vec_dot": ([vp, i, i, i, vpp, vpp, dp, vp], i),
         "tn_vec_random": ([vp, i, i, i, ctypes.c_uint64, vpp, vp], i),
+        "tn_vec_alloc": ([vp, i, i, i, vpp], i),
+        "tn_vec_free": ([i, vpp], None),
+        "tn_sync": ([vp], i),
         "tn_operator_set_stored_matrix_mode": ([vp, i, vp], i),
         "tn_gca_build": ([vp, vp, vp], i),
         "tn_operator_copy_local_matrices": ([vp, vp], i),
@@ -539,6 +542,31 @@ def vec_scale(shell: Shell, level: int, y, x, stream=None):
     _check(load().tn_vec_scale(shell.handle, level % shell.num_levels, _prec(cy[0].dtype), len(cy), _ptrs(cy),
                                _ptrs(cx), _stream(stream)))
     return y
+
+
+class DeviceVector:
+    """ncomp arrays of a level's nodes allocated by the library (tn_vec_alloc, zero-filled); `pointers` holds the
+    device addresses, released by tn_vec_free when the object goes away."""
+
+    def __init__(self, shell: Shell, level: int, ncomp: int, dtype=None):
+        import torch
+
+        self.shell, self.level, self.ncomp = shell, level % shell.num_levels, ncomp
+        self.dtype = dtype or torch.float64
+        arr = (ctypes.c_void_p * ncomp)()
+        _check(load().tn_vec_alloc(shell.handle, self.level, _prec(self.dtype), ncomp, arr))
+        self._arr = arr
+        self.pointers = [arr[c] for c in range(ncomp)]
+
+    def __del__(self):
+        if getattr(self, "_arr", None) is not None and _lib is not None:
+            _lib.tn_vec_free(self.ncomp, self._arr)
+            self._arr = None
+
+
+def sync(stream=None):
+    """tn_sync: wait for the stream's work."""
+    _check(load().tn_sync(_stream(stream)))
 
 
 def vec_max_abs(shell: Shell, level: int, a, stream=None) -> float:

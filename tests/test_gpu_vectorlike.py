@@ -108,3 +108,29 @@ def test_freeslip_penalty_matches_oracle(cuda):
     # the penalty (about 1e-7 of the input) dominates; rounding of A rot is ~1e-15 of a generic apply
     assert np.abs(out.cpu().numpy() - ref).max() < 1e-13 * np.abs(plain).max()
     assert np.abs(ref).max() > 1e3 * 1e-15 * np.abs(plain).max()
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_vec_alloc_free_and_sync(cuda, dtype):
+    """tn_vec_alloc gives zero-filled, 256-byte-aligned arrays of the level's nodes that the other entry points
+    accept; seeded values written into them read back through tn_vec_max_abs; tn_sync returns TN_OK."""
+    import ctypes
+
+    import torch
+
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    g = T.Shell(3, num_levels=2)
+    v = T.DeviceVector(g, 1, 3, dt)
+    assert all(p % 256 == 0 for p in v.pointers)
+    L = T.load()
+    prec = T.TN_F64 if dtype == "f64" else T.TN_F32
+    arr = (ctypes.c_void_p * 3)(*v.pointers)
+    out = ctypes.c_double()
+    assert L.tn_vec_max_abs(g.handle, 1, prec, 3, arr, ctypes.byref(out), None) == 0
+    assert out.value == 0.0
+    assert L.tn_vec_random(g.handle, 1, prec, 3, ctypes.c_uint64(7), arr, None) == 0
+    T.sync()
+    assert L.tn_vec_max_abs(g.handle, 1, prec, 3, arr, ctypes.byref(out), None) == 0
+    assert 0.5 < out.value <= 1.0  # uniform(-1, 1) over 3 x 10 x 9 x 9 x 9 values
+    del v
+    T.sync()

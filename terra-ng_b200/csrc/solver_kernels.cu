@@ -127,44 +127,67 @@ __device__ __forceinline__ void st_policy(double2* a, double2 v, uint64_t pol)
 
 // Gram-Schmidt step over pairs of entries (components start at multiples of
 // 64 entries, so pairs are 16-byte aligned); the odd tail entry is handled
-// by the thread that owns pair index n / 2.
+// by the thread that owns pair index n / 2. Each thread takes kMgsUnroll
+// grid-strided pairs per trip and issues all their loads before the first
+// store, so that enough bytes are in flight to cover DRAM latency; the pairs
+// are accumulated in the same order as a one-pair loop would.
+constexpr int kMgsUnroll = 2;
+
+// kSub: subtract h v_sub from w first (every step but the first);
+// kDot: dot with v_dot (every step but the last, which takes ||w||^2).
+template <bool kSub, bool kDot>
 __global__ void __launch_bounds__(kThreads) mgs_kernel(VecDesc L, double* __restrict__ w,
                                                         const double* __restrict__ vsub, const double* hsub,
                                                         const double* __restrict__ vdot, RedScratch rs, double* out,
                                                         int take_sqrt)
 {
-    const double   h      = vsub ? *hsub : 0.0;
-    const uint64_t pol    = l2_policy(vdot != nullptr);
+    const double   h      = kSub ? *hsub : 0.0;
+    const uint64_t pol    = l2_policy(kDot);
     double         acc    = 0.0;
     const int64_t  stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int s = 0; s < L.nseg; ++s) {
         const VecSeg  S  = L.seg[s];
         const int64_t np = S.n / 2;
         for (int c = 0; c < S.ncomp; ++c) {
-            const int64_t o  = S.offset + c * S.stride;
-            double2*      w2 = reinterpret_cast<double2*>(w + o);
-            const double2* s2 = vsub ? reinterpret_cast<const double2*>(vsub + o) : nullptr;
-            const double2* d2 = vdot ? reinterpret_cast<const double2*>(vdot + o) : nullptr;
-            for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < np; k += stride) {
-                double2 wv = ld_policy(w2 + k, pol);
-                if (s2) {
-                    const double2 sv = __ldcs(s2 + k);
-                    wv.x             = wv.x - h * sv.x;
-                    wv.y             = wv.y - h * sv.y;
-                    st_policy(w2 + k, wv, pol);
+            const int64_t  o  = S.offset + c * S.stride;
+            double2*       w2 = reinterpret_cast<double2*>(w + o);
+            const double2* s2 = reinterpret_cast<const double2*>(vsub + o);
+            const double2* d2 = reinterpret_cast<const double2*>(vdot + o);
+            for (int64_t k0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k0 < np;
+                 k0 += kMgsUnroll * stride) {
+                double2 wv[kMgsUnroll], sv[kMgsUnroll], dv[kMgsUnroll];
+#pragma unroll
+                for (int u = 0; u < kMgsUnroll; ++u) {
+                    const int64_t k = k0 + u * stride;
+                    if (k < np) {
+                        wv[u] = ld_policy(w2 + k, pol);
+                        if constexpr (kSub) sv[u] = __ldcs(s2 + k);
+                        if constexpr (kDot) dv[u] = __ldcs(d2 + k);
+                    }
                 }
-                const double2 dv = d2 ? __ldcs(d2 + k) : wv;
-                if (S.owned[lat_of(2 * k, S.rdiv)]) acc += wv.x * dv.x;
-                if (S.owned[lat_of(2 * k + 1, S.rdiv)]) acc += wv.y * dv.y;
+#pragma unroll
+                for (int u = 0; u < kMgsUnroll; ++u) {
+                    const int64_t k = k0 + u * stride;
+                    if (k < np) {
+                        if constexpr (kSub) {
+                            wv[u].x = wv[u].x - h * sv[u].x;
+                            wv[u].y = wv[u].y - h * sv[u].y;
+                            st_policy(w2 + k, wv[u], pol);
+                        }
+                        const double2 d = kDot ? dv[u] : wv[u];
+                        if (S.owned[lat_of(2 * k, S.rdiv)]) acc += wv[u].x * d.x;
+                        if (S.owned[lat_of(2 * k + 1, S.rdiv)]) acc += wv[u].y * d.y;
+                    }
+                }
             }
             if ((S.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
                 const int64_t i  = S.n - 1;
                 double        wi = w[o + i];
-                if (vsub) {
+                if constexpr (kSub) {
                     wi       = wi - h * vsub[o + i];
                     w[o + i] = wi;
                 }
-                if (S.owned[lat_of(i, S.rdiv)]) acc += wi * (vdot ? vdot[o + i] : wi);
+                if (S.owned[lat_of(i, S.rdiv)]) acc += wi * (kDot ? vdot[o + i] : wi);
             }
         }
     }
@@ -895,7 +918,14 @@ template int vec_dot<float>(const VecDesc&, const float*, const float*, double*,
 int mgs_step(const VecDesc& L, double* w, const double* v_sub, const double* h_sub, const double* v_dot, double* out,
              RedScratch rs, cudaStream_t st)
 {
-    mgs_kernel<<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, v_dot ? 0 : 1);
+    if (v_sub && v_dot)
+        mgs_kernel<true, true><<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, 0);
+    else if (v_dot)
+        mgs_kernel<false, true><<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, 0);
+    else if (v_sub)
+        mgs_kernel<true, false><<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, 1);
+    else
+        mgs_kernel<false, false><<<kBlocks, kThreads, 0, st>>>(L, w, v_sub, h_sub, v_dot, rs, out, 1);
     return launch_status();
 }
 

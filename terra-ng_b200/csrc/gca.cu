@@ -673,11 +673,11 @@ __global__ void __launch_bounds__(kN * kN) gca_bake_kernel(GcaBakeArgs A)
 }
 
 // Stored-matrix apply: dst += A src. One thread per (cell, wedge), cells
-// fastest so that each packed value is one coalesced load across a warp; the
-// matrix streams through L2 with evict-first loads (it is read once per apply)
-// while src / dst stay cached. The 171 packed entries are walked in a fully
-// unrolled loop whose (row, column) pairs are compile-time constants, keeping
-// the 18 inputs and 18 outputs in registers.
+// fastest so that each packed value is one coalesced load across a warp; on
+// large levels the matrix streams through L2 with evict-first loads (it is
+// read once per apply) while src / dst stay cached. The 171 packed entries are
+// walked in a fully unrolled loop whose (row, column) pairs are compile-time
+// constants, keeping the 18 inputs and 18 outputs in registers.
 template <typename T>
 struct GcaApplyArgs {
     int        nl, nr;
@@ -707,31 +707,40 @@ __host__ __device__ constexpr int pair_col(int p)
     return a + p;
 }
 
-template <typename T>
-__device__ __forceinline__ T ld_stream(const T* p)
+// Matrix loads: evict-first where a level's matrices are too large to stay in
+// L2 between applies (they are read once per apply); plain loads where they
+// fit, so that the consecutive applies of one smoothing sweep find them in L2
+// (the level-4 FP32 matrices of a level-6 hierarchy, 56 MB).
+constexpr int64_t kGcaStreamBytes = 64ll << 20;
+
+template <typename T, bool kStream>
+__device__ __forceinline__ T ld_mat(const T* p)
 {
-    return __ldcs(p);
+    if constexpr (kStream)
+        return __ldcs(p);
+    else
+        return __ldg(p);
 }
 
 // o += A s over packed entries P.. with compile-time (row, column)
-template <typename T, int P>
+template <typename T, bool kStream, int P>
 __device__ __forceinline__ void packed_matvec(const T* m, int64_t nc, const T (&s)[kN], T (&o)[kN])
 {
     if constexpr (P < kPack) {
         constexpr int a = pair_row(P), b = pair_col(P);
-        const T       v = ld_stream(m + static_cast<int64_t>(P) * nc);
+        const T       v = ld_mat<T, kStream>(m + static_cast<int64_t>(P) * nc);
         if constexpr (a == b) {
             o[a] += v * s[a];
         } else {
             o[a] += v * s[b];
             o[b] += v * s[a];
         }
-        packed_matvec<T, P + 1>(m, nc, s, o);
+        packed_matvec<T, kStream, P + 1>(m, nc, s, o);
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(128) gca_apply_kernel(GcaApplyArgs<T> A)
+template <typename T, bool kStream>
+__global__ void __launch_bounds__(128, 3) gca_apply_kernel(GcaApplyArgs<T> A)
 {
     const int nl = A.nl, nr = A.nr;
     const int nc  = A.cells ? A.nslots : 10 * (nl - 1) * (nl - 1) * (nr - 1);
@@ -752,7 +761,7 @@ __global__ void __launch_bounds__(128) gca_apply_kernel(GcaApplyArgs<T> A)
 #pragma unroll
     for (int a = 0; a < kN; ++a) o[a] = T(0);
     const T* m = A.mats + static_cast<int64_t>(w * kPack) * nc + cell;
-    packed_matvec<T, 0>(m, nc, s, o);
+    packed_matvec<T, kStream, 0>(m, nc, s, o);
 #pragma unroll
     for (int n = 0; n < 6; ++n)
 #pragma unroll
@@ -964,7 +973,12 @@ int gca_apply_add(int nl, int nr, const T* mats, const T* const* src, T* const* 
     a.nslots        = nslots;
     const int items = 2 * (cells ? nslots : 10 * (nl - 1) * (nl - 1) * (nr - 1));
     if (items == 0) return 0;
-    gca_apply_kernel<T><<<(items + 127) / 128, 128, 0, st>>>(a);
+    const bool stream = static_cast<int64_t>(items) * kPack * static_cast<int64_t>(sizeof(T)) > kGcaStreamBytes;
+    const int  blocks = (items + 127) / 128;
+    if (stream)
+        gca_apply_kernel<T, true><<<blocks, 128, 0, st>>>(a);
+    else
+        gca_apply_kernel<T, false><<<blocks, 128, 0, st>>>(a);
     return launch_status();
 }
 template int gca_apply_add<double>(int, int, const double*, const double* const*, double* const*, cudaStream_t,

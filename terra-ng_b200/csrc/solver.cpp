@@ -420,11 +420,19 @@ void VelocityMultigrid::apply(int l, const T* x, T* y, cudaStream_t st)
 }
 
 // Chebyshev::solve_impl (chebyshev.hpp:102-176); rho carries over between the
-// outer iterations as in the reference.
+// outer iterations as in the reference. With x_zero (x holds zeros on entry,
+// as in every pre-smoothing of a V-cycle that starts from zero) the first
+// step's A x is exactly zero and is written as zeros instead of applied.
 template <typename T>
-void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st)
+void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st, bool x_zero)
 {
     Work<T>& W = work<T>();
+    auto     residual_apply = [&](T* ax, bool first) {
+        if (first && x_zero)
+            cuda_check(cudaMemsetAsync(ax, 0, sizeof(T) * W.tmp[l].total(), st), "zero");
+        else
+            apply<T>(l, x, ax, st);
+    };
     if (opt_.smoother == 1) {
         // Jacobi::solve_impl (jacobi.hpp:51-60): x += omega D^-1 (b - A x), one
         // fused update per step (the first-step form of the Chebyshev kernel)
@@ -433,7 +441,7 @@ void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st)
         T*            d    = W.d[l].data();
         const T*      invd = W.invdiag[l].data();
         for (int it = 0; it < opt_.cheb_iters; ++it) {
-            apply<T>(l, x, ax, st);
+            residual_apply(ax, it == 0);
             chk(cheb_step<T>(n, x, d, b, ax, invd, static_cast<T>(opt_.jacobi_omega), T(0), true, st), "jacobi");
         }
         return;
@@ -449,7 +457,7 @@ void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st)
     T*            d     = W.d[l].data();
     const T*      invd  = W.invdiag[l].data();
     for (int it = 0; it < opt_.cheb_iters; ++it) {
-        apply<T>(l, x, ax, st);
+        residual_apply(ax, it == 0);
         chk(cheb_step<T>(n, x, d, b, ax, invd, static_cast<T>(1.0 / theta), T(0), true, st), "chebyshev");
         for (int i = 2; i <= opt_.cheb_order; ++i) {
             const double rho_new = 1.0 / (2.0 * sigma - rho);
@@ -465,7 +473,7 @@ void VelocityMultigrid::smooth(int l, T* x, const T* b, cudaStream_t st)
 
 // solve_recursive (multigrid.hpp:288-432, classical V-cycle branch)
 template <typename T>
-void VelocityMultigrid::vcycle(int l, T* x, const T* b, cudaStream_t st)
+void VelocityMultigrid::vcycle(int l, T* x, const T* b, cudaStream_t st, bool x_zero)
 {
     if (l == 0) {
         coarse_solve<T>(x, b, st);
@@ -474,7 +482,7 @@ void VelocityMultigrid::vcycle(int l, T* x, const T* b, cudaStream_t st)
     Work<T>&           W  = work<T>();
     const DeviceLevel& L  = sh_->level(l);
     const DeviceLevel& Lc = sh_->level(l - 1);
-    smooth<T>(l, x, b, st);
+    smooth<T>(l, x, b, st, x_zero);
     T* res = W.tmp[l].data();
     apply<T>(l, x, res, st);
     const T one_m[2] = {T(1), T(-1)};
@@ -492,14 +500,14 @@ void VelocityMultigrid::vcycle(int l, T* x, const T* b, cudaStream_t st)
         chk(restrict_owned<T>(L.nl(), L.nr(), 3, L.owned_lat.as<uint8_t>(), fin, cout, st), "restrict");
     chk(interface_sum<T>(Lc.iface, Lc.nr(), 3, cout, st), "interface sum");
     cuda_check(cudaMemsetAsync(ec, 0, sizeof(T) * W.e[l - 1].total(), st), "zero correction");
-    vcycle<T>(l - 1, ec, rc, st);
+    vcycle<T>(l - 1, ec, rc, st, true);
     const T* cin[3]  = {ec, ec + sc, ec + 2 * sc};
     T*       fout[3] = {x, x + sf, x + 2 * sf};
     if (opt_.transfer == 1)
         chk(prolongate_linear_add<T>(L.nl(), L.nr(), 3, L.linear_weights<T>(st), cin, fout, st), "prolongate");
     else
         chk(prolongate_add<T>(L.nl(), L.nr(), 3, cin, fout, st), "prolongate");
-    smooth<T>(l, x, b, st);
+    smooth<T>(l, x, b, st, false);
 }
 
 template <typename T>
@@ -555,15 +563,15 @@ void VelocityMultigrid::coarse_solve(T* x, const T* b, cudaStream_t st)
         chk(convert_f64_to_f32(nt, cx_.data(), reinterpret_cast<float*>(x), st), "narrow");
 }
 
-void VelocityMultigrid::solve64(double* x, const double* b, cudaStream_t st)
+void VelocityMultigrid::solve64(double* x, const double* b, cudaStream_t st, bool x_zero)
 {
-    for (int c = 0; c < opt_.num_vcycles; ++c) vcycle<double>(fine_, x, b, st);
+    for (int c = 0; c < opt_.num_vcycles; ++c) vcycle<double>(fine_, x, b, st, x_zero && c == 0);
 }
 
-void VelocityMultigrid::solve32(float* x, const float* b, cudaStream_t st)
+void VelocityMultigrid::solve32(float* x, const float* b, cudaStream_t st, bool x_zero)
 {
     if (!opt_.fp32) throw Error(kErrState, "the hierarchy was built without FP32 operators");
-    for (int c = 0; c < opt_.num_vcycles; ++c) vcycle<float>(fine_, x, b, st);
+    for (int c = 0; c < opt_.num_vcycles; ++c) vcycle<float>(fine_, x, b, st, x_zero && c == 0);
 }
 
 template <typename T>
@@ -728,11 +736,11 @@ void StokesSolver::precondition(const DVec<double>& v, DVec<double>& z, cudaStre
     if (opt_.mg.fp32) {
         chk(convert_f64_to_f32(t_.total(), t_.data(), t32_.data(), st), "narrow");
         cuda_check(cudaMemsetAsync(z32_.data(), 0, sizeof(float) * z32_.total(), st), "zero");
-        mg_->solve32(z32_.data(), t32_.data(), st);
+        mg_->solve32(z32_.data(), t32_.data(), st, true);
         chk(widen_check(z32_.total(), z32_.data(), z.data() + su.offset, scratch_.flag_dev(), st), "widen");
         chk(flag_nonfinite<double>(sp.stride, zp, scratch_.flag_dev(), st), "check");
     } else {
-        mg_->solve64(z.data() + su.offset, t_.data(), st);
+        mg_->solve64(z.data() + su.offset, t_.data(), st, true);  // both callers pass z = 0
         chk(flag_nonfinite<double>(z.total(), z.data(), scratch_.flag_dev(), st), "check");
     }
 }
@@ -1095,10 +1103,10 @@ void VelocitySolver::precondition(cudaStream_t st)
     if (opt_.mg.fp32) {
         chk(convert_f64_to_f32(r_.total(), r_.data(), r32_.data(), st), "narrow");
         cuda_check(cudaMemsetAsync(z32_.data(), 0, sizeof(float) * z32_.total(), st), "zero");
-        mg_->solve32(z32_.data(), r32_.data(), st);
+        mg_->solve32(z32_.data(), r32_.data(), st, true);
         chk(convert_f32_to_f64(z_.total(), z32_.data(), z_.data(), st), "widen");
     } else {
-        mg_->solve64(z_.data(), r_.data(), st);
+        mg_->solve64(z_.data(), r_.data(), st, true);
     }
 }
 

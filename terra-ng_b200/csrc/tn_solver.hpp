@@ -65,8 +65,9 @@ class VelocityMultigrid {
                       cudaStream_t st);
     // num_vcycles V-cycles on A x = b; x, b are velocity vectors (velocity_desc
     // layout) of the fine level in the precision of the call.
-    void solve64(double* x, const double* b, cudaStream_t st);
-    void solve32(float* x, const float* b, cudaStream_t st);
+    // x_zero: x holds zeros on entry (the first smoothing step then skips A x)
+    void solve64(double* x, const double* b, cudaStream_t st, bool x_zero = false);
+    void solve32(float* x, const float* b, cudaStream_t st, bool x_zero = false);
     double           lambda(int l) const { return lambda_.at(l); }
     const DVec<double>& inv_diag(int l) const { return w64_.invdiag.at(l); }
     EpsDivDivOp&     op64(int l) { return *ops64_.at(l); }
@@ -90,9 +91,9 @@ class VelocityMultigrid {
     template <typename T>
     void apply(int l, const T* x, T* y, cudaStream_t st);
     template <typename T>
-    void smooth(int l, T* x, const T* b, cudaStream_t st);
+    void smooth(int l, T* x, const T* b, cudaStream_t st, bool x_zero);
     template <typename T>
-    void vcycle(int l, T* x, const T* b, cudaStream_t st);
+    void vcycle(int l, T* x, const T* b, cudaStream_t st, bool x_zero);
     template <typename T>
     void coarse_solve(T* x, const T* b, cudaStream_t st);
     void build_dense_coarse(cudaStream_t st);  // kinv_ = inverse of the assembled coarsest operator

@@ -89,6 +89,30 @@ def test_multigrid_solver_history_matches_oracle(cuda, coarse):
     assert np.all(np.diff(hist) < 0) and hist[-1] < 0.1  # every V(2,2) cycle reduces the residual
 
 
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_zero_start_vcycle_skips_first_apply_exactly(cuda, mixed):
+    """The preconditioner starts its V-cycle from zero and writes the first pre-smoothing step's A x as zeros
+    instead of applying A; tn_solver_vcycle on x = 0 applies A to the zeros. With GCA off and the dense coarsest
+    solve no kernel on the path adds atomically, so the two results agree bit for bit (FP64, and the FP32 V-cycle
+    of the mixed solver on the narrowed right-hand side)."""
+    import torch
+
+    level, nlev, bcs = 4, 3, (1, 2)
+    sh = O.Shell(level)
+    k = smooth_viscosity(sh, 51, 100.0)
+    g = T.Shell(level, num_levels=nlev)
+    solver = T.VelocitySolver(g, eta=_t(k), bc_cmb=bcs[0], bc_surface=bcs[1], gca=0, mixed_precision=mixed,
+                              coarse_solver=T.COARSE_DENSE)
+    b = O.enforce_rhs_bcs(sh, consistent(sh, O.seeded_normal(sh.vec_shape, 52)), *bcs)
+    z = torch.zeros(sh.vec_shape, dtype=torch.float64, device=cuda)
+    solver.precondition(_t(b), z)
+    dt = torch.float32 if mixed else torch.float64
+    x = torch.zeros(sh.vec_shape, dtype=dt, device=cuda)
+    solver.vcycle(x, _t(b, dt))
+    assert float(z.abs().max()) > 0.0
+    assert torch.equal(z, x.double())
+
+
 def test_stokes_dense_coarse_reaches_tolerance(cuda):
     """The Stokes solve with the dense coarsest solve reaches 1e-8 and agrees with the reference-default
     (coarsest CG) solution."""

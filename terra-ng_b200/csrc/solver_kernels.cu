@@ -1107,8 +1107,6 @@ int pcg_config(int n, int nc, int nr, int ncls, int nmem, PcgConfig& out)
 }
 }  // namespace
 
-int coarse_pcg_cluster_size() { return pcg_cluster_size(coarse_pcg_kernel, 0); }
-
 int coarse_pcg_prepare(int nl, int nr, int num_classes, int num_members)
 {
     PcgConfig c;

@@ -342,6 +342,5 @@ int dense_coarse_prepare(int unknowns);
 // x = Kinv b (gathered at rep, scattered to every copy); y: 3 * nu doubles of scratch
 int dense_coarse_solve(int64_t nodes, int64_t stride, int nu, const int32_t* uid, const int32_t* rep,
                        const double* Kinv, const double* b, double* y, double* x, cudaStream_t st);
-int coarse_pcg_cluster_size();
 
 }  // namespace tn

@@ -48,6 +48,18 @@ def test_null_arguments_rejected():
     assert L.tn_vec_dot(None, 0, 0, 1, None, None, None, None) == -1
 
 
+def test_vec_alloc_and_free_argument_errors():
+    """tn_vec_alloc rejects a NULL shell or output array before touching the device; tn_vec_free skips a NULL
+    array and NULL entries (nothing to release)."""
+    L = T.load()
+    out = (ctypes.c_void_p * 4)()
+    assert L.tn_vec_alloc(None, 0, T.TN_F64, 3, out) == -1
+    assert b"NULL" in L.tn_last_error()
+    assert L.tn_vec_alloc(None, 0, T.TN_F64, 3, None) == -1
+    L.tn_vec_free(3, None)
+    L.tn_vec_free(4, (ctypes.c_void_p * 4)())
+
+
 def test_shell_create_without_device_fails_cleanly():
     import torch
 
